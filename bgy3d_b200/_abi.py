@@ -1,0 +1,117 @@
+"""ctypes binding of include/rism3d.h (librism3d.so, built in-tree).
+
+The library is the product: there is no Python or CPU fallback.  Importing
+this module raises if the shared object is missing.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librism3d.so")
+
+# Enumerations (rism3d.h)
+HNC, KH, PY = 0, 1, 2
+PSE0 = 3
+CLOSURES = {"HNC": 0, "KH": 1, "PY": 2, **{f"PSE{n}": 3 + n for n in range(8)}}
+NEWTON, PICARD, TRIAL = 0, 1, 2
+SOLVERS = {"newton": NEWTON, "picard": PICARD, "trial": TRIAL}
+FP64, MIXED = 0, 1
+
+OK = 0
+ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_TABLE, ERR_NOT_CONVERGED, ERR_NAN, ERR_UNSUPPORTED = range(-1, -8, -1)
+ERRORS = {
+    -1: "bad argument", -2: "CUDA error", -3: "out of device memory",
+    -4: "|k| beyond the chi table", -5: "not converged", -6: "NaN residual",
+    -7: "unsupported",
+}
+
+
+class Site(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 8), ("x", ctypes.c_double * 3),
+                ("sigma", ctypes.c_double), ("epsilon", ctypes.c_double),
+                ("charge", ctypes.c_double)]
+
+
+class Problem(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int * 3), ("L", ctypes.c_double * 3),
+                ("beta", ctypes.c_double), ("rho", ctypes.c_double),
+                ("rmax", ctypes.c_double), ("nrad", ctypes.c_int),
+                ("closure", ctypes.c_int), ("max_iter", ctypes.c_int),
+                ("norm_tol", ctypes.c_double), ("lambda_", ctypes.c_double),
+                ("solver", ctypes.c_int), ("renorm", ctypes.c_int),
+                ("precision", ctypes.c_int), ("verbosity", ctypes.c_int)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("mu", ctypes.c_double), ("mu_hnc", ctypes.c_double),
+                ("mu_kh", ctypes.c_double), ("mu_gf", ctypes.c_double),
+                ("pmv_factor", ctypes.c_double), ("resid_inf", ctypes.c_double),
+                ("resid_2", ctypes.c_double), ("status", ctypes.c_int),
+                ("newton_iters", ctypes.c_int), ("f_evals", ctypes.c_int),
+                ("jv_evals", ctypes.c_int), ("f_evals_fp32", ctypes.c_int),
+                ("jv_evals_fp32", ctypes.c_int), ("seconds", ctypes.c_double)]
+
+
+# Every entry point declared in include/rism3d.h (checked by the CPU tests).
+EXPORTS = [
+    "rism3d_problem_defaults", "rism3d_solute_solve", "rism3d_ctx_create",
+    "rism3d_ctx_destroy", "rism3d_ctx_size", "rism3d_iterate_t1",
+    "rism3d_jacobian_t1", "rism3d_iterate_t1_f32", "rism3d_jacobian_t1_f32",
+    "rism3d_solve", "rism3d_observables", "rism3d_get_field", "rism3d_last_error",
+    "rism3d_profile",
+]
+
+_lib = None
+
+
+def lib():
+    """Load librism3d.so once; raise if it is absent (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run `python -m bgy3d_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    P, I, D, V = ctypes.POINTER, ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+    L.rism3d_problem_defaults.argtypes = [P(Problem), D, I]
+    L.rism3d_problem_defaults.restype = None
+    L.rism3d_solute_solve.argtypes = [P(Problem), I, P(Site), I, P(Site), P(D), P(D), P(D), P(Result)]
+    L.rism3d_solute_solve.restype = I
+    L.rism3d_ctx_create.argtypes = [P(Problem), I, P(Site), I, P(Site), P(D), P(V)]
+    L.rism3d_ctx_create.restype = I
+    L.rism3d_ctx_destroy.argtypes = [V]
+    L.rism3d_ctx_destroy.restype = None
+    L.rism3d_ctx_size.argtypes = [V]
+    L.rism3d_ctx_size.restype = ctypes.c_longlong
+    for name in ("rism3d_iterate_t1", "rism3d_iterate_t1_f32"):
+        getattr(L, name).argtypes = [V, V, V, P(D)]
+        getattr(L, name).restype = I
+    for name in ("rism3d_jacobian_t1", "rism3d_jacobian_t1_f32"):
+        getattr(L, name).argtypes = [V, V, V, V]
+        getattr(L, name).restype = I
+    L.rism3d_solve.argtypes = [V, V, P(Result)]
+    L.rism3d_solve.restype = I
+    L.rism3d_observables.argtypes = [V, V, V, P(Result)]
+    L.rism3d_observables.restype = I
+    L.rism3d_get_field.argtypes = [V, I, V]
+    L.rism3d_get_field.restype = I
+    L.rism3d_last_error.argtypes = []
+    L.rism3d_last_error.restype = ctypes.c_char_p
+    L.rism3d_profile.argtypes = [V, I, P(D), P(ctypes.c_longlong)]
+    L.rism3d_profile.restype = I
+    _lib = L
+    return L
+
+
+class RismError(RuntimeError):
+    def __init__(self, code, where=""):
+        msg = ERRORS.get(code, f"error {code}")
+        detail = lib().rism3d_last_error().decode(errors="replace") if _lib else ""
+        super().__init__(f"{where}: {msg}" + (f" ({detail})" if detail else ""))
+        self.code = code
+
+
+def check(code, where):
+    if code != OK:
+        raise RismError(code, where)
+    return code

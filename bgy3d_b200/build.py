@@ -1,0 +1,48 @@
+"""Build librism3d.so (the C-ABI library of include/rism3d.h) in-tree for sm_100a.
+
+    python -m bgy3d_b200.build [--verbose-ptxas]
+
+nvcc cross-compiles without a GPU; the .so lands next to this file so it
+travels with the source tree.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "librism3d.so")
+SOURCES = ["rism3d.cu"]
+HEADERS = ["fft_core.cuh", "kernels.cuh"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+
+def _stale():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    deps.append(os.path.join(ROOT, "include", "rism3d.h"))
+    deps.append(os.path.abspath(__file__))
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force=False, verbose_ptxas=False):
+    if not force and not _stale() and not verbose_ptxas:
+        return LIB
+    cmd = [NVCC, "-O3", "-std=c++17", "-lineinfo",
+           "-gencode", "arch=compute_100a,code=sm_100a",
+           "-Xcompiler", "-fPIC,-O3", "-shared",
+           "-I", os.path.join(ROOT, "include"), "-I", CSRC,
+           "-o", LIB + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES]
+    if verbose_ptxas:
+        cmd.insert(1, "-Xptxas=-v")
+    subprocess.run(cmd, check=True)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force=True, verbose_ptxas="--verbose-ptxas" in sys.argv)
+    print(LIB)

@@ -1,0 +1,1084 @@
+// rism3d.cu -- host side of the B200-native 3D-RISM solute solver: the
+// C ABI of include/rism3d.h, the device-resident problem context, the
+// residual / Jacobian pipelines and the Newton-GMRES driver.
+//
+// Reference: hnc3d_solute_solve (hnc3d.c:1762-2350) driving iterate_t1 /
+// jacobian_t1 (hnc3d.c:1183-1362) through bgy3d_snes_newton
+// (bgy3d-snes.c:160-346, SNESNEWTONLS + KSPGMRES(30), KSP rtol = 100 * 1e-5).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "rism3d.h"
+
+using namespace rism;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct CudaFail {
+  int code;
+};
+
+#define CK(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) {                                                          \
+      g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);              \
+      throw CudaFail{e_ == cudaErrorMemoryAllocation ? RISM3D_ERR_NOMEM : RISM3D_ERR_CUDA}; \
+    }                                                                                 \
+  } while (0)
+
+#define CKL()                                                                         \
+  do {                                                                                \
+    cudaError_t e_ = cudaGetLastError();                                              \
+    if (e_ != cudaSuccess) {                                                          \
+      g_last_error = std::string("kernel launch: ") + cudaGetErrorString(e_);         \
+      throw CudaFail{RISM3D_ERR_CUDA};                                                \
+    }                                                                                 \
+  } while (0)
+
+struct ArgFail {
+  int code;
+  std::string msg;
+};
+
+template <typename T> T *dalloc(size_t count) {
+  void *p = nullptr;
+  if (count == 0) count = 1;
+  CK(cudaMalloc(&p, count * sizeof(T)));
+  return static_cast<T *>(p);
+}
+
+bool is_2a3b(int n) {
+  if (n <= 0) return false;
+  while (n % 2 == 0) n /= 2;
+  while (n % 3 == 0) n /= 3;
+  return n == 1;
+}
+
+AxisPlan make_plan(int n) {
+  AxisPlan p{};
+  p.n = n;
+  int m = n, s = 0;
+  while (m % 4 == 0) { p.rad[s++] = 4; m /= 4; }
+  while (m % 2 == 0) { p.rad[s++] = 2; m /= 2; }
+  while (m % 3 == 0) { p.rad[s++] = 3; m /= 3; }
+  p.nst = s;
+  return p;
+}
+
+// exp(-2 pi i q / n) in extended precision, rounded once.
+void twiddles(int n, std::vector<double2> &t64, std::vector<float2> &t32) {
+  t64.resize(n);
+  t32.resize(n);
+  const long double pi = 3.141592653589793238462643383279502884L;
+  for (int q = 0; q < n; ++q) {
+    const long double a = 2.0L * pi * (long double)q / (long double)n;
+    const long double c = cosl(a), s = -sinl(a);
+    t64[q] = make_double2((double)c, (double)s);
+    t32[q] = make_float2((float)c, (float)s);
+  }
+}
+
+// The radial interpolation rule of bgy3d-vec.c:22-46 as (value, slope)
+// pairs: f(x) = tab[i] + slope[i] * (x/dx - 1/2 - i), i = nearest entry.
+void interp_pairs(const double *tab, int n, std::vector<double2> &out) {
+  out.resize(n);
+  for (int i = 0; i < n; ++i) {
+    const int ip = (i < n - 2) ? i + 1 : i;
+    const int im = (i > 0 + 1) ? i - 1 : i;
+    const double fi = (tab[ip] - tab[im]) / (ip - im);
+    out[i] = make_double2(tab[i], fi);
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- context
+// Tile shapes of the passes: RX rows per x-pass CTA, BY / BZ kx-columns per
+// y / z-pass CTA; chosen so that n * batch <= reg_complex * 256 threads.
+struct TileShape {
+  int RX = 16, BY = 8, BZ = 8;
+};
+
+struct PassTimer {
+  bool on = false;
+  cudaEvent_t a, b;
+  double ms[8] = {0};
+  long long launches[8] = {0};
+};
+
+struct rism3d_ctx {
+  rism3d_problem pd;
+  int m = 0, n = 0;
+  Geo g{};
+  long long nvec = 0;  // m * Nr
+  TileShape tiles[2];  // [0]: FP64 passes, [1]: FP32 passes
+  std::vector<rism3d_site> solvent, solute;
+  std::vector<double> charge;
+  double h3 = 0, dkr = 0;
+
+  AxisPlan px64{}, py64{}, pz64{}, px32{}, py32{}, pz32{};
+  double2 *tw64[3] = {nullptr, nullptr, nullptr};
+  float2 *tw32[3] = {nullptr, nullptr, nullptr};
+  double2 *post64 = nullptr;
+  float2 *post32 = nullptr;
+
+  double *v64 = nullptr;
+  float *v32 = nullptr;
+  double2 *L64 = nullptr;
+  float2 *L32 = nullptr;
+  double2 *chi64 = nullptr, *s64 = nullptr;
+  float2 *chi32 = nullptr, *s32 = nullptr;
+  void *W = nullptr;  // complex work buffer, FP64-sized, reused by the FP32 path
+  SiteP *d_solute = nullptr;
+  double *d_charge = nullptr;
+
+  NormPartial *npart = nullptr;
+  std::vector<NormPartial> h_npart;
+  double *dpart = nullptr;
+  std::vector<double> h_dpart;
+  int red_blocks = 1184;
+
+  // solver work (lazily allocated)
+  double *F64 = nullptr, *X64t = nullptr, *F64t = nullptr;
+  float *X32 = nullptr, *F32 = nullptr, *X32t = nullptr, *F32t = nullptr;
+  double *d64 = nullptr;
+  float *d32 = nullptr;
+  std::vector<double *> basis64;
+  std::vector<float *> basis32;
+  double *dx64 = nullptr;
+  float *dx32 = nullptr;
+
+  cudaStream_t stream = 0;
+  PassTimer timer;
+  int f_evals = 0, jv_evals = 0, f32_evals = 0, jv32_evals = 0;
+
+  ~rism3d_ctx() {
+    auto fr = [](void *p) { if (p) cudaFree(p); };
+    for (int i = 0; i < 3; ++i) { fr(tw64[i]); fr(tw32[i]); }
+    fr(post64); fr(post32); fr(v64); fr(v32); fr(L64); fr(L32);
+    fr(chi64); fr(s64); fr(chi32); fr(s32); fr(W); fr(d_solute); fr(d_charge);
+    fr(npart); fr(dpart); fr(F64); fr(X64t); fr(F64t); fr(X32); fr(F32); fr(X32t); fr(F32t);
+    fr(d64); fr(d32); fr(dx64); fr(dx32);
+    for (auto p : basis64) fr(p);
+    for (auto p : basis32) fr(p);
+    if (timer.on) { cudaEventDestroy(timer.a); cudaEventDestroy(timer.b); }
+  }
+
+  template <typename T> const AxisPlan &plan(int axis) const;
+  template <typename T> typename Cx<T>::type *work() { return static_cast<typename Cx<T>::type *>(W); }
+  template <typename T> const TileShape &tl() const { return tiles[sizeof(T) == 8 ? 0 : 1]; }
+};
+
+template <> const AxisPlan &rism3d_ctx::plan<double>(int a) const { return a == 0 ? px64 : (a == 1 ? py64 : pz64); }
+template <> const AxisPlan &rism3d_ctx::plan<float>(int a) const { return a == 0 ? px32 : (a == 1 ? py32 : pz32); }
+
+namespace {
+
+enum { TK_XFWD = 0, TK_Y = 1, TK_Z = 2, TK_XINV = 3, TK_VEC = 4 };
+
+struct TimeScope {
+  rism3d_ctx *c;
+  int which;
+  TimeScope(rism3d_ctx *c_, int w) : c(c_), which(w) {
+    if (c->timer.on) cudaEventRecord(c->timer.a, c->stream);
+  }
+  ~TimeScope() {
+    if (c->timer.on) {
+      cudaEventRecord(c->timer.b, c->stream);
+      cudaEventSynchronize(c->timer.b);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, c->timer.a, c->timer.b);
+      c->timer.ms[which] += ms;
+      c->timer.launches[which] += 1;
+    }
+  }
+};
+
+template <typename T> ZParams<T> zparams(rism3d_ctx *c, bool full);
+template <> ZParams<double> zparams<double>(rism3d_ctx *c, bool full) {
+  ZParams<double> z{};
+  z.chi = c->chi64;
+  z.stab = (full && c->pd.renorm) ? c->s64 : nullptr;
+  z.L = full ? c->L64 : nullptr;
+  z.nrad = c->pd.nrad;
+  z.dkr = c->dkr;
+  for (int i = 0; i < c->m; ++i) {
+    z.a[i] = c->pd.renorm ? 0.0 : c->pd.beta * c->charge[i];
+    z.bconst[i] = c->pd.renorm ? 0.0 : c->pd.beta * c->charge[i];
+  }
+  return z;
+}
+template <> ZParams<float> zparams<float>(rism3d_ctx *c, bool full) {
+  ZParams<float> z{};
+  z.chi = c->chi32;
+  z.stab = (full && c->pd.renorm) ? c->s32 : nullptr;
+  z.L = full ? c->L32 : nullptr;
+  z.nrad = c->pd.nrad;
+  z.dkr = c->dkr;
+  for (int i = 0; i < c->m; ++i) {
+    z.a[i] = c->pd.renorm ? 0.f : (float)(c->pd.beta * c->charge[i]);
+    z.bconst[i] = c->pd.renorm ? 0.f : (float)(c->pd.beta * c->charge[i]);
+  }
+  return z;
+}
+
+template <typename T> const T *vfield(rism3d_ctx *c);
+template <> const double *vfield<double>(rism3d_ctx *c) { return c->v64; }
+template <> const float *vfield<float>(rism3d_ctx *c) { return c->v32; }
+template <typename T> const typename Cx<T>::type *postw(rism3d_ctx *c);
+template <> const double2 *postw<double>(rism3d_ctx *c) { return c->post64; }
+template <> const float2 *postw<float>(rism3d_ctx *c) { return c->post32; }
+
+template <typename T> size_t xsmem(rism3d_ctx *c) {
+  return sizeof(typename Cx<T>::type) * (size_t)(c->g.M + c->tl<T>().RX * c->g.M);
+}
+template <typename T> size_t ysmem(rism3d_ctx *c) {
+  return sizeof(typename Cx<T>::type) * (size_t)(c->g.N1 + c->g.N1 * c->tl<T>().BY);
+}
+template <typename T> size_t zsmem(rism3d_ctx *c) {
+  return sizeof(typename Cx<T>::type) * (size_t)(c->g.N2 + c->g.N2 * c->m * c->tl<T>().BZ);
+}
+
+template <typename T, bool INV> void launch_y(rism3d_ctx *c) {
+  TimeScope ts(c, TK_Y);
+  dim3 grid((c->g.Nh + c->tl<T>().BY - 1) / c->tl<T>().BY, c->g.N2, c->m);
+  const size_t sm = ysmem<T>(c);
+  auto *W = c->work<T>();
+  if (c->tl<T>().BY == 16) k_y<T, INV, 16><<<grid, 256, sm, c->stream>>>(c->g, c->plan<T>(1), W);
+  else if (c->tl<T>().BY == 8) k_y<T, INV, 8><<<grid, 256, sm, c->stream>>>(c->g, c->plan<T>(1), W);
+  else k_y<T, INV, 4><<<grid, 256, sm, c->stream>>>(c->g, c->plan<T>(1), W);
+  CKL();
+}
+
+template <typename T, int MODE> void launch_z(rism3d_ctx *c) {
+  TimeScope ts(c, TK_Z);
+  dim3 grid((c->g.Nh + c->tl<T>().BZ - 1) / c->tl<T>().BZ, c->g.N1);
+  const size_t sm = zsmem<T>(c);
+  auto *W = c->work<T>();
+  const ZParams<T> zp = zparams<T>(c, MODE == MODE_F);
+  if (c->tl<T>().BZ == 16) k_z<T, MODE, 16><<<grid, 256, sm, c->stream>>>(c->g, c->plan<T>(2), W, zp);
+  else if (c->tl<T>().BZ == 8) k_z<T, MODE, 8><<<grid, 256, sm, c->stream>>>(c->g, c->plan<T>(2), W, zp);
+  else k_z<T, MODE, 4><<<grid, 256, sm, c->stream>>>(c->g, c->plan<T>(2), W, zp);
+  CKL();
+}
+
+void reduce_norms(rism3d_ctx *c, int nblk, double *resid) {
+  c->h_npart.resize(nblk);
+  CK(cudaMemcpyAsync(c->h_npart.data(), c->npart, sizeof(NormPartial) * nblk, cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double amax = 0.0, s2 = 0.0;
+  for (int i = 0; i < nblk; ++i) {
+    const double a = c->h_npart[i].amax;
+    amax = (a > amax || a != a) ? a : amax;
+    s2 += c->h_npart[i].sum2;
+  }
+  resid[0] = amax;
+  resid[1] = std::sqrt(s2);
+}
+
+// F(x) -> out (iterate_t1).  resid: ||out||_inf, ||out||_2 (host), or null.
+template <typename T> void eval_F(rism3d_ctx *c, const T *x, T *out, double *resid) {
+  const int rows = c->g.N1 * c->g.N2;
+  dim3 gx((rows + c->tl<T>().RX - 1) / c->tl<T>().RX, c->m);
+  auto *W = c->work<T>();
+  {
+    TimeScope ts(c, TK_XFWD);
+    k_xfwd<T, MODE_F><<<gx, 256, xsmem<T>(c), c->stream>>>(c->g, c->plan<T>(0), c->tl<T>().RX, x, vfield<T>(c),
+                                                          (T)c->pd.beta, c->pd.closure, W, postw<T>(c));
+    CKL();
+  }
+  launch_y<T, false>(c);
+  launch_z<T, MODE_F>(c);
+  launch_y<T, true>(c);
+  {
+    TimeScope ts(c, TK_XINV);
+    k_xinv<T><<<gx, 256, xsmem<T>(c), c->stream>>>(c->g, c->plan<T>(0), c->tl<T>().RX, W, x, out,
+                                                   (T)(1.0 / (double)c->g.Nr), (T)1, postw<T>(c), c->npart);
+    CKL();
+  }
+  if (sizeof(T) == 8) c->f_evals++; else c->f32_evals++;
+  if (resid) reduce_norms(c, gx.x * gx.y, resid);
+}
+
+// out = J(x0) (s * vin) with d = c'(x0) precomputed (jacobian_t1).
+template <typename T> void eval_J(rism3d_ctx *c, const T *d, const T *vin, double s, T *out, double *resid) {
+  const int rows = c->g.N1 * c->g.N2;
+  dim3 gx((rows + c->tl<T>().RX - 1) / c->tl<T>().RX, c->m);
+  auto *W = c->work<T>();
+  {
+    TimeScope ts(c, TK_XFWD);
+    k_xfwd<T, MODE_J><<<gx, 256, xsmem<T>(c), c->stream>>>(c->g, c->plan<T>(0), c->tl<T>().RX, vin, d, (T)s,
+                                                          c->pd.closure, W, postw<T>(c));
+    CKL();
+  }
+  launch_y<T, false>(c);
+  launch_z<T, MODE_J>(c);
+  launch_y<T, true>(c);
+  {
+    TimeScope ts(c, TK_XINV);
+    k_xinv<T><<<gx, 256, xsmem<T>(c), c->stream>>>(c->g, c->plan<T>(0), c->tl<T>().RX, W, vin, out,
+                                                   (T)(1.0 / (double)c->g.Nr), (T)s, postw<T>(c), c->npart);
+    CKL();
+  }
+  if (sizeof(T) == 8) c->jv_evals++; else c->jv32_evals++;
+  if (resid) reduce_norms(c, gx.x * gx.y, resid);
+}
+
+int vec_grid(long long n) {
+  long long b = (n + 255) / 256;
+  return (int)std::min<long long>(b, 148LL * 8);
+}
+
+template <typename T> VecRef<T> vref(const T *p, double s) { return VecRef<T>{p, s}; }
+
+// h[i] = <w * ws, s_i V_i> for i < nv.
+template <typename T>
+void mdot(rism3d_ctx *c, const T *w, double ws, const std::vector<VecRef<T>> &V, std::vector<double> &h) {
+  TimeScope ts(c, TK_VEC);
+  const int nv = (int)V.size();
+  h.assign(nv, 0.0);
+  const int G = c->red_blocks;
+  for (int base = 0; base < nv; base += kDotChunk) {
+    VecRef<T> r[kDotChunk];
+    const int k = std::min(kDotChunk, nv - base);
+    for (int i = 0; i < kDotChunk; ++i) r[i] = i < k ? V[base + i] : V[base];
+    k_mdot<T><<<G, 256, 0, c->stream>>>(c->nvec, w, ws, k, r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7],
+                                         c->dpart);
+    CKL();
+    c->h_dpart.resize((size_t)G * kDotChunk);
+    CK(cudaMemcpyAsync(c->h_dpart.data(), c->dpart, sizeof(double) * G * kDotChunk, cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int b = 0; b < G; ++b)
+      for (int i = 0; i < k; ++i) h[base + i] += c->h_dpart[(size_t)b * kDotChunk + i];
+  }
+}
+
+// w = ws * w - sum_i coef_i (s_i V_i); returns ||w||_2 if want_norm.
+template <typename T>
+double maxpy(rism3d_ctx *c, T *w, double ws, const std::vector<VecRef<T>> &V, const std::vector<double> &coef,
+             bool want_norm) {
+  TimeScope ts(c, TK_VEC);
+  const int nv = (int)V.size();
+  const int G = c->red_blocks;
+  double *dcoef = c->dpart + (size_t)G * kDotChunk;  // scratch after the partials
+  double norm = 0.0;
+  if (nv == 0) {
+    VecRef<T> r0 = vref<T>(w, 0.0);
+    k_maxpy<T><<<G, 256, 0, c->stream>>>(c->nvec, w, ws, 0, r0, r0, r0, r0, r0, r0, r0, r0, dcoef,
+                                          want_norm ? c->dpart : nullptr);
+    CKL();
+  }
+  for (int base = 0; base < nv; base += kDotChunk) {
+    const int k = std::min(kDotChunk, nv - base);
+    VecRef<T> r[kDotChunk];
+    for (int i = 0; i < kDotChunk; ++i) r[i] = i < k ? V[base + i] : V[base];
+    CK(cudaMemcpyAsync(dcoef, coef.data() + base, sizeof(double) * k, cudaMemcpyHostToDevice, c->stream));
+    const bool last = base + kDotChunk >= nv;
+    k_maxpy<T><<<G, 256, 0, c->stream>>>(c->nvec, w, base == 0 ? ws : 1.0, k, r[0], r[1], r[2], r[3], r[4],
+                                          r[5], r[6], r[7], dcoef, (last && want_norm) ? c->dpart : nullptr);
+    CKL();
+  }
+  if (want_norm) {
+    c->h_dpart.resize(G);
+    CK(cudaMemcpyAsync(c->h_dpart.data(), c->dpart, sizeof(double) * G, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    double s = 0.0;
+    for (int b = 0; b < G; ++b) s += c->h_dpart[b];
+    norm = std::sqrt(s);
+  } else {
+    CK(cudaStreamSynchronize(c->stream));  // coef upload buffer is reused
+  }
+  return norm;
+}
+
+template <typename TX, typename TY> void axpby(rism3d_ctx *c, double a, const TX *x, double b, TY *y) {
+  TimeScope ts(c, TK_VEC);
+  k_axpby<TX, TY><<<vec_grid(c->nvec), 256, 0, c->stream>>>(c->nvec, a, x, b, y);
+  CKL();
+}
+template <typename TX, typename TY, typename TZ>
+void xpay(rism3d_ctx *c, const TX *x, double a, const TY *y, TZ *z) {
+  TimeScope ts(c, TK_VEC);
+  k_xpay<TX, TY, TZ><<<vec_grid(c->nvec), 256, 0, c->stream>>>(c->nvec, x, a, y, z);
+  CKL();
+}
+
+template <typename T> std::vector<T *> &basis(rism3d_ctx *c);
+template <> std::vector<double *> &basis<double>(rism3d_ctx *c) { return c->basis64; }
+template <> std::vector<float *> &basis<float>(rism3d_ctx *c) { return c->basis32; }
+
+template <typename T> void ensure_basis(rism3d_ctx *c, int count) {
+  auto &B = basis<T>(c);
+  while ((int)B.size() < count) B.push_back(dalloc<T>(c->nvec));
+}
+
+// GMRES(restart) without preconditioner for J x = b, x0 = 0 (KSPGMRES with
+// classical Gram-Schmidt, PCNONE; bgy3d-snes.c:262-306).  Returns the
+// number of J.v products.  b is overwritten.
+template <typename T>
+int gmres(rism3d_ctx *c, const T *d, T *b, T *x, double rtol, int maxit, int restart) {
+  ensure_basis<T>(c, restart + 1);
+  auto &B = basis<T>(c);
+  std::vector<double> H((size_t)(restart + 1) * restart), cs(restart), sn(restart), gv(restart + 1);
+  std::vector<VecRef<T>> V;
+  std::vector<double> h;
+  int its = 0;
+  bool have_x = false;
+  double beta0 = -1.0;
+  while (its < maxit) {
+    // r = b - J x (first cycle: r = b)
+    double resid[2];
+    if (!have_x) {
+      axpby<T, T>(c, 1.0, b, 0.0, B[0]);
+      V.assign(1, vref<T>(B[0], 1.0));
+      const double nb = maxpy<T>(c, B[0], 1.0, {}, {}, true);
+      resid[1] = nb;
+    } else {
+      eval_J<T>(c, d, x, 1.0, B[0], nullptr);  // B0 = J x
+      xpay<T, T, T>(c, b, -1.0, B[0], B[0]);   // B0 = b - J x
+      resid[1] = maxpy<T>(c, B[0], 1.0, {}, {}, true);
+      its++;
+    }
+    const double beta = resid[1];
+    if (beta0 < 0) beta0 = beta;
+    if (beta == 0.0 || beta <= rtol * beta0) break;
+    V.assign(1, vref<T>(B[0], 1.0 / beta));
+    std::fill(gv.begin(), gv.end(), 0.0);
+    gv[0] = beta;
+    int j = 0;
+    bool done = false;
+    for (; j < restart && its < maxit; ++j) {
+      eval_J<T>(c, d, V[j].p, V[j].s, B[j + 1], nullptr);
+      its++;
+      mdot<T>(c, B[j + 1], 1.0, V, h);
+      const double hn = maxpy<T>(c, B[j + 1], 1.0, V, h, true);
+      for (int i = 0; i <= j; ++i) H[(size_t)i * restart + j] = h[i];
+      H[(size_t)(j + 1) * restart + j] = hn;
+      for (int i = 0; i < j; ++i) {  // previous Givens rotations
+        const double a = H[(size_t)i * restart + j], bb = H[(size_t)(i + 1) * restart + j];
+        H[(size_t)i * restart + j] = cs[i] * a + sn[i] * bb;
+        H[(size_t)(i + 1) * restart + j] = -sn[i] * a + cs[i] * bb;
+      }
+      const double a = H[(size_t)j * restart + j], bb = H[(size_t)(j + 1) * restart + j];
+      const double r = std::hypot(a, bb);
+      cs[j] = r == 0.0 ? 1.0 : a / r;
+      sn[j] = r == 0.0 ? 0.0 : bb / r;
+      H[(size_t)j * restart + j] = r;
+      H[(size_t)(j + 1) * restart + j] = 0.0;
+      gv[j + 1] = -sn[j] * gv[j];
+      gv[j] = cs[j] * gv[j];
+      V.push_back(vref<T>(B[j + 1], hn > 0.0 ? 1.0 / hn : 0.0));
+      if (std::fabs(gv[j + 1]) <= rtol * beta0 || hn == 0.0) { ++j; done = true; break; }
+    }
+    // y = H^-1 g, x += sum y_i V_i
+    const int k = j;
+    std::vector<double> y(k);
+    for (int i = k - 1; i >= 0; --i) {
+      double s = gv[i];
+      for (int l = i + 1; l < k; ++l) s -= H[(size_t)i * restart + l] * y[l];
+      y[i] = H[(size_t)i * restart + i] != 0.0 ? s / H[(size_t)i * restart + i] : 0.0;
+    }
+    std::vector<VecRef<T>> Vk(V.begin(), V.begin() + k);
+    std::vector<double> my(k);
+    for (int i = 0; i < k; ++i) my[i] = -y[i];
+    maxpy<T>(c, x, have_x ? 1.0 : 0.0, Vk, my, false);
+    have_x = true;
+    if (done) break;
+  }
+  if (!have_x) axpby<T, T>(c, 0.0, b, 0.0, x);
+  return its;
+}
+
+template <typename T> T *xbuf(rism3d_ctx *c, int which);
+template <> double *xbuf<double>(rism3d_ctx *c, int w) {
+  double **p = w == 0 ? &c->F64 : (w == 1 ? &c->X64t : &c->F64t);
+  if (!*p) *p = dalloc<double>(c->nvec);
+  return *p;
+}
+template <> float *xbuf<float>(rism3d_ctx *c, int w) {
+  float **p = w == 0 ? &c->F32 : (w == 1 ? &c->X32t : &c->F32t);
+  if (!*p) *p = dalloc<float>(c->nvec);
+  return *p;
+}
+template <typename T> T *slopebuf(rism3d_ctx *c);
+template <> double *slopebuf<double>(rism3d_ctx *c) { if (!c->d64) c->d64 = dalloc<double>(c->nvec); return c->d64; }
+template <> float *slopebuf<float>(rism3d_ctx *c) { if (!c->d32) c->d32 = dalloc<float>(c->nvec); return c->d32; }
+template <typename T> T *dxbuf(rism3d_ctx *c);
+template <> double *dxbuf<double>(rism3d_ctx *c) { if (!c->dx64) c->dx64 = dalloc<double>(c->nvec); return c->dx64; }
+template <> float *dxbuf<float>(rism3d_ctx *c) { if (!c->dx32) c->dx32 = dalloc<float>(c->nvec); return c->dx32; }
+
+template <typename TS> __global__ void k_slope_any(long long n, const TS *__restrict__ t, const double *__restrict__ v,
+                                                   double beta, int closure, float *__restrict__ d32,
+                                                   double *__restrict__ d64) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const double d = closure_d<double>(closure, beta * v[p], (double)t[p]);
+  if (d32) d32[p] = (float)d;
+  if (d64) d64[p] = d;
+}
+
+template <typename TS, typename TJ> void closure_slope(rism3d_ctx *c, const TS *x, TJ *d) {
+  TimeScope ts(c, TK_VEC);
+  const long long n = c->nvec;
+  float *d32 = sizeof(TJ) == 4 ? reinterpret_cast<float *>(d) : nullptr;
+  double *d64 = sizeof(TJ) == 8 ? reinterpret_cast<double *>(d) : nullptr;
+  k_slope_any<TS><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, x, c->v64, c->pd.beta, c->pd.closure,
+                                                                       d32, d64);
+  CKL();
+}
+
+struct NewtonOut {
+  int iters = 0;
+  double rinf = 0, r2 = 0;
+  bool converged = false;
+  bool nan = false;
+  bool stalled = false;
+};
+
+// Inexact Newton with backtracking (SNESNEWTONLS, bgy3d-snes.c:160-346):
+// state and residual in TS, Jacobian products and Krylov basis in TJ.
+// Stops when ||F||_inf < tol.
+template <typename TS, typename TJ>
+NewtonOut newton(rism3d_ctx *c, TS *x, double tol, int max_iter, double krylov_rtol, int restart) {
+  NewtonOut o;
+  TS *F = xbuf<TS>(c, 0);
+  TS *xt = xbuf<TS>(c, 1);
+  TS *Ft = xbuf<TS>(c, 2);
+  TJ *d = slopebuf<TJ>(c);
+  TJ *dx = dxbuf<TJ>(c);
+  // -F in the Jacobian precision: Ft doubles as scratch when TS == TJ,
+  // otherwise the (idle) FP32 trial buffer
+  TJ *rhs = xbuf<TJ>(c, sizeof(TJ) == sizeof(TS) ? 2 : 1);
+  double r[2];
+  eval_F<TS>(c, x, F, r);
+  for (int it = 0;; ++it) {
+    o.rinf = r[0];
+    o.r2 = r[1];
+    if (c->pd.verbosity > 0)
+      std::fprintf(stderr, " # newton<%s,%s> %3d: |F|inf = %.3e |F|2 = %.3e\n", sizeof(TS) == 8 ? "f64" : "f32",
+                   sizeof(TJ) == 8 ? "f64" : "f32", it, r[0], r[1]);
+    if (!(r[0] == r[0]) || !(r[1] == r[1]) || std::isinf(r[0])) { o.nan = true; break; }
+    if (r[0] < tol) { o.converged = true; break; }
+    if (it >= max_iter) break;
+    o.iters = it + 1;
+    closure_slope<TS, TJ>(c, x, d);
+    axpby<TS, TJ>(c, -1.0, F, 0.0, rhs);
+    gmres<TJ>(c, d, rhs, dx, krylov_rtol, 1000, restart);
+    const double f0 = r[1] * r[1];
+    double lam = 1.0, f1 = 0.0, rt[2] = {0, 0};
+    bool decreased = false;
+    for (int ls = 0; ls < 20; ++ls) {
+      xpay<TS, TJ, TS>(c, x, lam, dx, xt);
+      eval_F<TS>(c, xt, Ft, rt);
+      f1 = rt[1] * rt[1];
+      if (f1 <= (1.0 - 2e-4 * lam) * f0) { decreased = true; break; }
+      if (!(f1 == f1)) break;
+      double ln = lam * lam * f0 / (f1 - f0 + 2.0 * lam * f0);
+      ln = std::min(std::max(ln, 0.1 * lam), 0.5 * lam);
+      lam = ln;
+    }
+    if (!decreased) {  // SNES_DIVERGED_LINE_SEARCH: keep the last accepted x
+      o.stalled = true;
+      break;
+    }
+    // accept: x <- xt, F <- Ft
+    axpby<TS, TS>(c, 1.0, xt, 0.0, x);
+    axpby<TS, TS>(c, 1.0, Ft, 0.0, F);
+    r[0] = rt[0];
+    r[1] = rt[1];
+  }
+  return o;
+}
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+int solve_impl(rism3d_ctx *c, double *T, rism3d_result *out) {
+  rism3d_result res{};
+  c->f_evals = c->jv_evals = c->f32_evals = c->jv32_evals = 0;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, c->stream));
+  const double krtol = 1e-3;  // 100 * PETSc default rtol 1e-5 (bgy3d-snes.c:277)
+  const int restart = 30;
+  NewtonOut o;
+  int status = RISM3D_OK;
+  const rism3d_problem &pd = c->pd;
+  if (pd.closure == RISM3D_PY && pd.solver != RISM3D_PICARD) {
+    CK(cudaEventDestroy(e0));
+    CK(cudaEventDestroy(e1));
+    return RISM3D_ERR_UNSUPPORTED;
+  }
+  if (pd.solver == RISM3D_PICARD || pd.solver == RISM3D_TRIAL) {
+    // bgy3d_snes_picard (bgy3d-snes.c:348-384): x += lambda F(x).
+    const int steps = pd.solver == RISM3D_TRIAL ? 100 : pd.max_iter;
+    const double lam = pd.solver == RISM3D_TRIAL ? 0.02 : pd.lambda;
+    double *F = xbuf<double>(c, 0);
+    double r[2] = {0, 0};
+    for (int k = 0; k < steps; ++k) {
+      eval_F<double>(c, T, F, r);
+      xpay<double, double, double>(c, T, lam, F, T);
+      o.iters = k + 1;
+      if (r[0] < pd.norm_tol) { o.converged = true; break; }
+    }
+    o.rinf = r[0];
+    o.r2 = r[1];
+  }
+  if (pd.solver != RISM3D_PICARD) {
+    if (pd.precision == RISM3D_MIXED) {
+      // FP32 bulk: Newton on a float copy of t until the float residual floor.
+      if (!c->X32) c->X32 = dalloc<float>(c->nvec);
+      axpby<double, float>(c, 1.0, T, 0.0, c->X32);
+      const double tol32 = std::max(pd.norm_tol, 2e-4);
+      NewtonOut a = newton<float, float>(c, c->X32, tol32, pd.max_iter, krtol, restart);
+      axpby<float, double>(c, 1.0, c->X32, 0.0, T);
+      // FP64 residual with FP32 Jacobian: iterative refinement to norm_tol.
+      o = newton<double, float>(c, T, pd.norm_tol, pd.max_iter, krtol, restart);
+      o.iters += a.iters;
+    } else {
+      o = newton<double, double>(c, T, pd.norm_tol, pd.max_iter, krtol, restart);
+    }
+  }
+  CK(cudaEventRecord(e1, c->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  CK(cudaEventDestroy(e0));
+  CK(cudaEventDestroy(e1));
+  if (o.nan) status = RISM3D_ERR_NAN;
+  else if (!o.converged) status = RISM3D_ERR_NOT_CONVERGED;
+  res.status = status;
+  res.newton_iters = o.iters;
+  res.resid_inf = o.rinf;
+  res.resid_2 = o.r2;
+  res.f_evals = c->f_evals;
+  res.jv_evals = c->jv_evals;
+  res.f_evals_fp32 = c->f32_evals;
+  res.jv_evals_fp32 = c->jv32_evals;
+  res.seconds = ms * 1e-3;
+  if (out) {
+    const double keep[5] = {out->mu, out->mu_hnc, out->mu_kh, out->mu_gf, out->pmv_factor};
+    *out = res;
+    out->mu = keep[0]; out->mu_hnc = keep[1]; out->mu_kh = keep[2]; out->mu_gf = keep[3];
+    out->pmv_factor = keep[4];
+  }
+  return status;
+}
+
+int observables_impl(rism3d_ctx *c, const double *T, double *g, rism3d_result *out) {
+  const Geo &G = c->g;
+  double *uc = dalloc<double>(G.Nr);
+  const rism3d_problem &pd = c->pd;
+  const double h0 = pd.L[0] / pd.N[0], h1 = pd.L[1] / pd.N[1], h2 = pd.L[2] / pd.N[2];
+  const unsigned nb = (unsigned)((G.Nr + 255) / 256);
+  k_coulomb_long<<<nb, 256, 0, c->stream>>>(G, h0, h1, h2, pd.L[0], pd.L[1], pd.L[2], c->n, c->d_solute, uc);
+  CKL();
+  ObsPartial *part = dalloc<ObsPartial>(nb);
+  k_observables<<<nb, 256, 0, c->stream>>>(G, T, c->v64, uc, pd.beta, pd.closure, c->d_charge, g, part);
+  CKL();
+  std::vector<ObsPartial> hp(nb);
+  CK(cudaMemcpyAsync(hp.data(), part, sizeof(ObsPartial) * nb, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFree(part);
+  cudaFree(uc);
+  double s[5] = {0, 0, 0, 0, 0};
+  for (unsigned b = 0; b < nb; ++b) {
+    s[0] += hp[b].mu; s[1] += hp[b].hnc; s[2] += hp[b].kh; s[3] += hp[b].gf; s[4] += hp[b].csum;
+  }
+  // mu = rho * sum * h^3 / beta (chempot, hnc3d.c:604-623); PMV 1 - rho h^3 sum c
+  const double f = pd.rho * c->h3 / pd.beta;
+  if (out) {
+    out->mu = s[0] * f;
+    out->mu_hnc = s[1] * f;
+    out->mu_kh = s[2] * f;
+    out->mu_gf = s[3] * f;
+    out->pmv_factor = 1.0 - s[4] * (pd.rho * c->h3);
+  }
+  return RISM3D_OK;
+}
+
+int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int n, const rism3d_site *solute,
+                const double *chi, rism3d_ctx **out) {
+  if (!pd || !solvent || (!solute && n > 0) || !chi || !out) throw ArgFail{RISM3D_ERR_ARG, "null argument"};
+  if (m < 1 || m > kMaxSites) throw ArgFail{RISM3D_ERR_ARG, "solvent sites must be 1..6"};
+  if (n < 0) throw ArgFail{RISM3D_ERR_ARG, "negative solute size"};
+  for (int d = 0; d < 3; ++d) {
+    if (!is_2a3b(pd->N[d]) || pd->N[d] % 2 || pd->N[d] < 8 || pd->N[d] > kMaxN)
+      throw ArgFail{RISM3D_ERR_ARG, "N must be even 2^a 3^b in [8, 512]"};
+    if (!(pd->L[d] > 0)) throw ArgFail{RISM3D_ERR_ARG, "L must be positive"};
+  }
+  if (pd->nrad < 4 || !(pd->rmax > 0)) throw ArgFail{RISM3D_ERR_ARG, "bad radial grid"};
+  if (pd->closure < 0 || pd->closure > RISM3D_PSE7) throw ArgFail{RISM3D_ERR_ARG, "no such closure"};
+  auto c = new rism3d_ctx();
+  try {
+    c->pd = *pd;
+    c->m = m;
+    c->n = n;
+    c->solvent.assign(solvent, solvent + m);
+    c->solute.assign(solute, solute + n);
+    Geo &G = c->g;
+    G.N0 = pd->N[0]; G.N1 = pd->N[1]; G.N2 = pd->N[2];
+    G.M = G.N0 / 2;
+    G.Nh = G.M + 1;
+    G.Nhp = (G.Nh + 1) & ~1;
+    G.m = m;
+    G.Nr = (long long)G.N0 * G.N1 * G.N2;
+    G.Nc = (long long)G.Nhp * G.N1 * G.N2;
+    const double pi = 3.14159265358979323846;
+    G.dk0 = 2 * pi / pd->L[0];
+    G.dk1 = 2 * pi / pd->L[1];
+    G.dk2 = 2 * pi / pd->L[2];
+    c->nvec = (long long)m * G.Nr;
+    const double h0 = pd->L[0] / pd->N[0], h1 = pd->L[1] / pd->N[1], h2 = pd->L[2] / pd->N[2];
+    c->h3 = h0 * h1 * h2;
+    c->dkr = pi / pd->rmax;
+    // tile shapes per precision: n * batch <= reg_complex * 256 threads
+    for (int pr = 0; pr < 2; ++pr) {
+      const int rc = pr == 0 ? reg_complex<double2>() : reg_complex<float2>();
+      TileShape &t = c->tiles[pr];
+      t.RX = 32;
+      while (t.RX > 1 && G.M * t.RX > rc * 256) t.RX /= 2;
+      t.BY = 16;
+      while (t.BY > 4 && G.N1 * t.BY > rc * 256) t.BY /= 2;
+      t.BZ = 16;
+      while (t.BZ > 4 && G.N2 * t.BZ > rc * 256) t.BZ /= 2;
+      if (G.N1 * t.BY > rc * 256 || G.N2 * t.BZ > rc * 256)
+        throw ArgFail{RISM3D_ERR_ARG, "grid too large for the tile shapes"};
+    }
+    // |k| of every grid point must fall inside the chi table (interp assert,
+    // bgy3d-vec.c:30-31)
+    const double kmax = std::sqrt(std::pow(G.M * G.dk0, 2) + std::pow(G.N1 / 2 * G.dk1, 2) +
+                                  std::pow(G.N2 / 2 * G.dk2, 2));
+    if ((int)(kmax / c->dkr - 0.5 + 0.5) >= pd->nrad) throw ArgFail{RISM3D_ERR_TABLE, "chi table too short"};
+    for (int i = 0; i < m; ++i) c->charge.push_back(solvent[i].charge);
+
+    // FFT plans and twiddles
+    const int lens[3] = {G.M, G.N1, G.N2};
+    for (int a = 0; a < 3; ++a) {
+      std::vector<double2> t64;
+      std::vector<float2> t32;
+      twiddles(lens[a], t64, t32);
+      c->tw64[a] = dalloc<double2>(lens[a]);
+      c->tw32[a] = dalloc<float2>(lens[a]);
+      CK(cudaMemcpy(c->tw64[a], t64.data(), sizeof(double2) * lens[a], cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(c->tw32[a], t32.data(), sizeof(float2) * lens[a], cudaMemcpyHostToDevice));
+    }
+    c->px64 = make_plan(G.M); c->px64.tw = c->tw64[0];
+    c->py64 = make_plan(G.N1); c->py64.tw = c->tw64[1];
+    c->pz64 = make_plan(G.N2); c->pz64.tw = c->tw64[2];
+    c->px32 = c->px64; c->px32.tw = c->tw32[0];
+    c->py32 = c->py64; c->py32.tw = c->tw32[1];
+    c->pz32 = c->pz64; c->pz32.tw = c->tw32[2];
+    {
+      std::vector<double2> t64;
+      std::vector<float2> t32;
+      twiddles(G.N0, t64, t32);  // post twiddles exp(-2 pi i k / N0), k in [0, M]
+      c->post64 = dalloc<double2>(G.Nh);
+      c->post32 = dalloc<float2>(G.Nh);
+      CK(cudaMemcpy(c->post64, t64.data(), sizeof(double2) * G.Nh, cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(c->post32, t32.data(), sizeof(float2) * G.Nh, cudaMemcpyHostToDevice));
+    }
+    // radial tables: chi - delta (solvent_kernel_rism, hnc3d.c:1548-1556) and
+    // beta/eps0 s_i (rism_solvent_renorm, rism.f90:141-208)
+    const int nrad = pd->nrad;
+    const int npair = m * (m + 1) / 2;
+    std::vector<double2> chi64((size_t)npair * nrad), s64((size_t)m * nrad);
+    std::vector<double> tab(nrad);
+    std::vector<double2> pr;
+    for (int i = 0; i < m; ++i)
+      for (int j = 0; j <= i; ++j) {
+        for (int k = 0; k < nrad; ++k) tab[k] = chi[((size_t)i * m + j) * nrad + k] - (i == j ? 1.0 : 0.0);
+        interp_pairs(tab.data(), nrad, pr);
+        std::copy(pr.begin(), pr.end(), chi64.begin() + (size_t)(i * (i + 1) / 2 + j) * nrad);
+      }
+    const double dk = pi / pd->rmax;
+    for (int i = 0; i < m; ++i) {
+      std::vector<double> x(nrad, 0.0);
+      for (int j = 0; j < m; ++j)
+        for (int k = 0; k < nrad; ++k) x[k] = x[k] + chi[((size_t)j * m + i) * nrad + k] * solvent[j].charge;
+      for (int k = 0; k < nrad; ++k) {
+        const double kk = (2 * (k + 1) - 1) * dk / 2;
+        const double v = kk == 0.0 ? 0.0 : 4 * pi * std::exp(-kk * kk / (4 * kG * kG)) / (kk * kk);
+        tab[k] = pd->beta * kEps0Inv * (x[k] * v);
+      }
+      interp_pairs(tab.data(), nrad, pr);
+      std::copy(pr.begin(), pr.end(), s64.begin() + (size_t)i * nrad);
+    }
+    std::vector<float2> chi32(chi64.size()), s32(s64.size());
+    for (size_t i = 0; i < chi64.size(); ++i) chi32[i] = make_float2((float)chi64[i].x, (float)chi64[i].y);
+    for (size_t i = 0; i < s64.size(); ++i) s32[i] = make_float2((float)s64[i].x, (float)s64[i].y);
+    c->chi64 = dalloc<double2>(chi64.size());
+    c->chi32 = dalloc<float2>(chi32.size());
+    c->s64 = dalloc<double2>(s64.size());
+    c->s32 = dalloc<float2>(s32.size());
+    CK(cudaMemcpy(c->chi64, chi64.data(), sizeof(double2) * chi64.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->chi32, chi32.data(), sizeof(float2) * chi32.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->s64, s64.data(), sizeof(double2) * s64.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->s32, s32.data(), sizeof(float2) * s32.size(), cudaMemcpyHostToDevice));
+
+    // sites
+    std::vector<SiteP> hs(std::max(n, 1)), hv(m);
+    for (int u = 0; u < n; ++u)
+      hs[u] = SiteP{solute[u].x[0], solute[u].x[1], solute[u].x[2], solute[u].sigma, solute[u].epsilon,
+                    solute[u].charge};
+    for (int i = 0; i < m; ++i)
+      hv[i] = SiteP{solvent[i].x[0], solvent[i].x[1], solvent[i].x[2], solvent[i].sigma, solvent[i].epsilon,
+                    solvent[i].charge};
+    c->d_solute = dalloc<SiteP>(std::max(n, 1));
+    CK(cudaMemcpy(c->d_solute, hs.data(), sizeof(SiteP) * std::max(n, 1), cudaMemcpyHostToDevice));
+    SiteP *d_solvent = dalloc<SiteP>(m);
+    CK(cudaMemcpy(d_solvent, hv.data(), sizeof(SiteP) * m, cudaMemcpyHostToDevice));
+    c->d_charge = dalloc<double>(m);
+    CK(cudaMemcpy(c->d_charge, c->charge.data(), sizeof(double) * m, cudaMemcpyHostToDevice));
+
+    // fields
+    c->v64 = dalloc<double>(c->nvec);
+    c->v32 = dalloc<float>(c->nvec);
+    const unsigned nb = (unsigned)((G.Nr + 255) / 256);
+    k_field0<<<nb, 256>>>(G, h0, h1, h2, pd->L[0], pd->L[1], pd->L[2], d_solvent, n, c->d_solute, c->v64);
+    CKL();
+    k_axpby<double, float><<<vec_grid(c->nvec), 256>>>(c->nvec, 1.0, c->v64, 0.0, c->v32);
+    CKL();
+    c->L64 = dalloc<double2>((size_t)G.Nc);
+    c->L32 = dalloc<float2>((size_t)G.Nc);
+    CK(cudaMemset(c->L64, 0, sizeof(double2) * (size_t)G.Nhp * G.N1 * G.N2));
+    CK(cudaMemset(c->L32, 0, sizeof(float2) * (size_t)G.Nhp * G.N1 * G.N2));
+    const long long nk = (long long)G.Nh * G.N1 * G.N2;
+    k_longrange<<<(unsigned)((nk + 255) / 256), 256>>>(G, n, c->d_solute, pd->renorm, 1.0 / c->h3, c->L64,
+                                                       c->L32);
+    CKL();
+    CK(cudaDeviceSynchronize());
+    cudaFree(d_solvent);
+    CK(cudaMalloc(&c->W, sizeof(double2) * (size_t)(m * G.Nc)));
+    c->dpart = dalloc<double>((size_t)c->red_blocks * kDotChunk + 64);
+    const int rows = G.N1 * G.N2;
+    const int rxmin = std::min(c->tiles[0].RX, c->tiles[1].RX);
+    c->npart = dalloc<NormPartial>((size_t)((rows + rxmin - 1) / rxmin) * m);
+    // shared-memory opt-in
+    const size_t sx64 = xsmem<double>(c), sy64 = ysmem<double>(c), sz64 = zsmem<double>(c);
+    const int big = 227 * 1024;
+    if (sx64 > (size_t)big || sy64 > (size_t)big || sz64 > (size_t)big)
+      throw ArgFail{RISM3D_ERR_ARG, "tile exceeds shared memory"};
+    CK(cudaFuncSetAttribute(k_xfwd<double, MODE_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_xfwd<double, MODE_J>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_xfwd<float, MODE_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_xfwd<float, MODE_J>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_xinv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    CK(cudaFuncSetAttribute(k_xinv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+#define OPTIN_YZ(T)                                                                                    \
+  CK(cudaFuncSetAttribute(k_y<T, false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));   \
+  CK(cudaFuncSetAttribute(k_y<T, true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));    \
+  CK(cudaFuncSetAttribute(k_y<T, false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));    \
+  CK(cudaFuncSetAttribute(k_y<T, true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));     \
+  CK(cudaFuncSetAttribute(k_y<T, false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));    \
+  CK(cudaFuncSetAttribute(k_y<T, true, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));     \
+  CK(cudaFuncSetAttribute(k_z<T, MODE_F, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));  \
+  CK(cudaFuncSetAttribute(k_z<T, MODE_J, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));  \
+  CK(cudaFuncSetAttribute(k_z<T, MODE_F, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));   \
+  CK(cudaFuncSetAttribute(k_z<T, MODE_J, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));   \
+  CK(cudaFuncSetAttribute(k_z<T, MODE_F, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));   \
+  CK(cudaFuncSetAttribute(k_z<T, MODE_J, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    OPTIN_YZ(double)
+    OPTIN_YZ(float)
+#undef OPTIN_YZ
+  } catch (...) {
+    delete c;
+    throw;
+  }
+  *out = c;
+  return RISM3D_OK;
+}
+
+template <typename F> int guard(F &&f) {
+  try {
+    return f();
+  } catch (const CudaFail &e) {
+    return e.code;
+  } catch (const ArgFail &e) {
+    g_last_error = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    g_last_error = "host allocation failed";
+    return RISM3D_ERR_NOMEM;
+  }
+}
+
+}  // namespace
+
+// ================================================================== C ABI
+extern "C" {
+
+void rism3d_problem_defaults(rism3d_problem *pd, double L_half, int N) {
+  std::memset(pd, 0, sizeof(*pd));
+  for (int d = 0; d < 3; ++d) {
+    pd->N[d] = N;
+    pd->L[d] = 2 * L_half;
+  }
+  pd->beta = 1.6889;
+  pd->rho = 0.033427745;
+  pd->rmax = 2 * L_half / 2;
+  pd->nrad = N;
+  pd->closure = RISM3D_HNC;
+  pd->max_iter = 1500;
+  pd->norm_tol = 1.0e-7;
+  pd->lambda = 0.02;
+  pd->solver = RISM3D_NEWTON;
+  pd->renorm = 1;
+  pd->precision = RISM3D_FP64;
+  pd->verbosity = 0;
+}
+
+const char *rism3d_last_error(void) { return g_last_error.c_str(); }
+
+int rism3d_ctx_create(const rism3d_problem *pd, int m, const rism3d_site *solvent, int n,
+                      const rism3d_site *solute, const double *chi, rism3d_ctx **ctx) {
+  if (ctx) *ctx = nullptr;
+  return guard([&] { return create_impl(pd, m, solvent, n, solute, chi, ctx); });
+}
+
+void rism3d_ctx_destroy(rism3d_ctx *ctx) { delete ctx; }
+
+long long rism3d_ctx_size(const rism3d_ctx *ctx) { return ctx ? ctx->nvec : 0; }
+
+int rism3d_iterate_t1(rism3d_ctx *ctx, const double *T, double *dT, double *resid) {
+  if (!ctx || !T || !dT) return RISM3D_ERR_ARG;
+  return guard([&] {
+    double r[2];
+    eval_F<double>(ctx, T, dT, r);
+    if (resid) resid[0] = r[0], resid[1] = r[1];
+    return RISM3D_OK;
+  });
+}
+
+int rism3d_jacobian_t1(rism3d_ctx *ctx, const double *T, const double *dT, double *JdT) {
+  if (!ctx || !T || !dT || !JdT) return RISM3D_ERR_ARG;
+  if (ctx->pd.closure == RISM3D_PY) return RISM3D_ERR_UNSUPPORTED;
+  return guard([&] {
+    double *d = slopebuf<double>(ctx);
+    closure_slope<double, double>(ctx, T, d);
+    eval_J<double>(ctx, d, dT, 1.0, JdT, nullptr);
+    CK(cudaStreamSynchronize(ctx->stream));
+    return RISM3D_OK;
+  });
+}
+
+int rism3d_iterate_t1_f32(rism3d_ctx *ctx, const float *T, float *dT, double *resid) {
+  if (!ctx || !T || !dT) return RISM3D_ERR_ARG;
+  return guard([&] {
+    double r[2];
+    eval_F<float>(ctx, T, dT, r);
+    if (resid) resid[0] = r[0], resid[1] = r[1];
+    return RISM3D_OK;
+  });
+}
+
+int rism3d_jacobian_t1_f32(rism3d_ctx *ctx, const float *T, const float *dT, float *JdT) {
+  if (!ctx || !T || !dT || !JdT) return RISM3D_ERR_ARG;
+  if (ctx->pd.closure == RISM3D_PY) return RISM3D_ERR_UNSUPPORTED;
+  return guard([&] {
+    float *d = slopebuf<float>(ctx);
+    closure_slope<float, float>(ctx, T, d);
+    eval_J<float>(ctx, d, dT, 1.0, JdT, nullptr);
+    CK(cudaStreamSynchronize(ctx->stream));
+    return RISM3D_OK;
+  });
+}
+
+int rism3d_solve(rism3d_ctx *ctx, double *T, rism3d_result *out) {
+  if (!ctx || !T) return RISM3D_ERR_ARG;
+  return guard([&] { return solve_impl(ctx, T, out); });
+}
+
+int rism3d_observables(rism3d_ctx *ctx, const double *T, double *g, rism3d_result *out) {
+  if (!ctx || !T) return RISM3D_ERR_ARG;
+  return guard([&] { return observables_impl(ctx, T, g, out); });
+}
+
+int rism3d_get_field(rism3d_ctx *ctx, int which, double *dst) {
+  if (!ctx || !dst) return RISM3D_ERR_ARG;
+  return guard([&] {
+    if (which == 0) {
+      CK(cudaMemcpy(dst, ctx->v64, sizeof(double) * ctx->nvec, cudaMemcpyDeviceToDevice));
+    } else if (which == 1) {
+      const rism3d_problem &pd = ctx->pd;
+      const unsigned nb = (unsigned)((ctx->g.Nr + 255) / 256);
+      k_coulomb_long<<<nb, 256, 0, ctx->stream>>>(ctx->g, pd.L[0] / pd.N[0], pd.L[1] / pd.N[1], pd.L[2] / pd.N[2],
+                                                  pd.L[0], pd.L[1], pd.L[2], ctx->n, ctx->d_solute, dst);
+      CKL();
+      CK(cudaStreamSynchronize(ctx->stream));
+    } else {
+      return (int)RISM3D_ERR_ARG;
+    }
+    return (int)RISM3D_OK;
+  });
+}
+
+int rism3d_solute_solve(const rism3d_problem *pd, int m, const rism3d_site *solvent, int n,
+                        const rism3d_site *solute, const double *chi, double *t_inout, double *g_out,
+                        rism3d_result *out) {
+  rism3d_ctx *ctx = nullptr;
+  int rc = rism3d_ctx_create(pd, m, solvent, n, solute, chi, &ctx);
+  if (rc != RISM3D_OK) {
+    if (out) { std::memset(out, 0, sizeof(*out)); out->status = rc; }
+    return rc;
+  }
+  rc = guard([&] {
+    const size_t bytes = sizeof(double) * ctx->nvec;
+    double *T = dalloc<double>(ctx->nvec);
+    double *g = g_out ? dalloc<double>(ctx->nvec) : nullptr;
+    struct Free { double *a, *b; ~Free() { if (a) cudaFree(a); if (b) cudaFree(b); } } fr{T, g};
+    if (t_inout) CK(cudaMemcpy(T, t_inout, bytes, cudaMemcpyHostToDevice));
+    else CK(cudaMemset(T, 0, bytes));
+    rism3d_result r{};
+    int st = solve_impl(ctx, T, &r);
+    observables_impl(ctx, T, g, &r);
+    r.status = st;
+    if (t_inout) CK(cudaMemcpy(t_inout, T, bytes, cudaMemcpyDeviceToHost));
+    if (g_out) CK(cudaMemcpy(g_out, g, bytes, cudaMemcpyDeviceToHost));
+    if (out) *out = r;
+    return st;
+  });
+  rism3d_ctx_destroy(ctx);
+  if (out && rc < 0 && out->status == 0) out->status = rc;
+  return rc;
+}
+
+// ---- profiling hooks (per-pass CUDA-event timing, off by default) -------
+int rism3d_profile(rism3d_ctx *ctx, int on, double *ms_out, long long *launches_out) {
+  if (!ctx) return RISM3D_ERR_ARG;
+  return guard([&] {
+    if (ms_out)
+      for (int i = 0; i < 5; ++i) ms_out[i] = ctx->timer.ms[i];
+    if (launches_out)
+      for (int i = 0; i < 5; ++i) launches_out[i] = ctx->timer.launches[i];
+    if (on && !ctx->timer.on) {
+      CK(cudaEventCreate(&ctx->timer.a));
+      CK(cudaEventCreate(&ctx->timer.b));
+      ctx->timer.on = true;
+    } else if (!on && ctx->timer.on) {
+      cudaEventDestroy(ctx->timer.a);
+      cudaEventDestroy(ctx->timer.b);
+      ctx->timer.on = false;
+    }
+    for (int i = 0; i < 8; ++i) ctx->timer.ms[i] = 0, ctx->timer.launches[i] = 0;
+    return (int)RISM3D_OK;
+  });
+}
+
+}  // extern "C"

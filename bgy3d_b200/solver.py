@@ -1,0 +1,214 @@
+"""Host-side mirror of the reference's hnc3d solute interface over the C ABI.
+
+``hnc3d_run_solute(solute, solvent, settings, chi, restart)`` mirrors the
+Scheme procedure ``hnc3d-run-solute`` (guile/bgy3d.scm:386-388) and its C
+body ``hnc3d_solute_solve`` (hnc3d.c:1762-2350): it returns the result
+dictionary the reference conses up (``free-energy``,
+``partial-molar-volume-factor``, ``GUV`` = g, ``RESTART`` = t), and raises
+on non-convergence where the reference longjmps through scm_misc_error
+(bgy3d-snes.c:338-345).
+
+``RismContext`` exposes the inner plug points -- the VecFunc1/VecFunc2
+callbacks iterate_t1 / jacobian_t1 (hnc3d.c:1183-1362) -- on
+device-resident torch tensors.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _abi
+
+# Settings as in the reference's *defaults* (guile/bgy3d.scm:323-340) and
+# problem_data (bgy3d-guile.c:243-386).
+DEFAULTS = {
+    "L": 10.0, "N": 64, "rho": 0.033427745, "beta": 1.6889, "norm-tol": 1.0e-7,
+    "max-iter": 1500, "lambda": 0.02, "closure": "HNC", "snes-solver": "newton",
+    "no-renorm": False, "precision": "fp64", "verbosity": 0,
+}
+
+
+def problem_data(settings):
+    """ProblemData from a settings dict (bgy3d-guile.c:243-386).
+
+    ``L`` is the HALF box edge as in the reference (L[i] = 2 * length);
+    rmax/nrad default to max(L)/2 and max(N) of the full box."""
+    s = dict(DEFAULTS)
+    s.update(settings or {})
+    pd = _abi.Problem()
+    n = s["N"]
+    N = tuple(n) if isinstance(n, (tuple, list)) else (int(n),) * 3
+    Lh = s["L"]
+    Lfull = tuple(2.0 * float(x) for x in Lh) if isinstance(Lh, (tuple, list)) else (2.0 * float(Lh),) * 3
+    for d in range(3):
+        pd.N[d] = int(N[d])
+        pd.L[d] = Lfull[d]
+    pd.beta = float(s["beta"])
+    pd.rho = float(s["rho"])
+    pd.rmax = float(s.get("rmax", max(Lfull) / 2))
+    pd.nrad = int(s.get("nrad", max(N)))
+    cl = s["closure"]
+    pd.closure = _abi.CLOSURES[cl] if isinstance(cl, str) else int(cl)
+    pd.max_iter = int(s["max-iter"])
+    pd.norm_tol = float(s["norm-tol"])
+    pd.lambda_ = float(s["lambda"])
+    pd.solver = _abi.SOLVERS[s["snes-solver"]]
+    pd.renorm = 0 if s["no-renorm"] else 1
+    pd.precision = {"fp64": _abi.FP64, "mixed": _abi.MIXED}[s["precision"]]
+    pd.verbosity = int(s["verbosity"])
+    return pd
+
+
+def _sites(sites):
+    arr = (_abi.Site * max(1, len(sites)))()
+    for i, s in enumerate(sites):
+        arr[i].name = s.get("name", "X").encode()[:7]
+        for d in range(3):
+            arr[i].x[d] = float(s["x"][d])
+        arr[i].sigma = float(s["sigma"])
+        arr[i].epsilon = float(s["epsilon"])
+        arr[i].charge = float(s["charge"])
+    return arr
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _result_dict(r):
+    return {
+        "free-energy": r.mu, "mu-hnc": r.mu_hnc, "mu-kh": r.mu_kh, "mu-gf": r.mu_gf,
+        "partial-molar-volume-factor": r.pmv_factor, "resid-inf": r.resid_inf, "resid-2": r.resid_2,
+        "status": r.status, "newton-iters": r.newton_iters, "f-evals": r.f_evals,
+        "jv-evals": r.jv_evals, "f-evals-fp32": r.f_evals_fp32, "jv-evals-fp32": r.jv_evals_fp32,
+        "seconds": r.seconds,
+    }
+
+
+def hnc3d_run_solute(solute, solvent, settings, chi, restart=None, want_g=True):
+    """One 3D-RISM solute solve with host buffers (rism3d_solute_solve).
+
+    chi: [m][m][nrad] solvent susceptibility (not offset by one) on the
+    radial k-grid (p + 1/2) pi / rmax; settings must then carry the rmax and
+    nrad it was computed with.  restart: initial t [m][N2][N1][N0] or None.
+    """
+    L = _abi.lib()
+    pd = problem_data(settings)
+    m, n = len(solvent), len(solute)
+    chi = np.ascontiguousarray(chi, dtype=np.float64)
+    if chi.shape != (m, m, pd.nrad):
+        raise ValueError(f"chi must be [{m}][{m}][{pd.nrad}], got {chi.shape}")
+    shape = (m, pd.N[2], pd.N[1], pd.N[0])
+    t = np.zeros(shape) if restart is None else np.array(restart, dtype=np.float64, order="C", copy=True)
+    if t.shape != shape:
+        raise ValueError("restart has the wrong shape")
+    g = np.empty(shape) if want_g else None
+    res = _abi.Result()
+    rc = L.rism3d_solute_solve(ctypes.byref(pd), m, _sites(solvent), n, _sites(solute), _dptr(chi),
+                               _dptr(t), _dptr(g) if g is not None else None, ctypes.byref(res))
+    out = _result_dict(res)
+    if rc != _abi.OK and rc != _abi.ERR_NOT_CONVERGED:
+        raise _abi.RismError(rc, "hnc3d_run_solute")
+    if rc == _abi.ERR_NOT_CONVERGED:
+        raise _abi.RismError(rc, "hnc3d_run_solute")
+    out["GUV"] = g
+    out["RESTART"] = t
+    return out
+
+
+class RismContext:
+    """Device-resident problem (rism3d_ctx) on the current CUDA device."""
+
+    def __init__(self, solute, solvent, settings, chi):
+        import torch  # device memory only
+        self._torch = torch
+        L = _abi.lib()
+        self.pd = problem_data(settings)
+        self.m, self.n = len(solvent), len(solute)
+        chi = np.ascontiguousarray(chi, dtype=np.float64)
+        if chi.shape != (self.m, self.m, self.pd.nrad):
+            raise ValueError("chi has the wrong shape")
+        self._chi = chi
+        h = ctypes.c_void_p()
+        _abi.check(L.rism3d_ctx_create(ctypes.byref(self.pd), self.m, _sites(solvent), self.n,
+                                       _sites(solute), _dptr(chi), ctypes.byref(h)), "rism3d_ctx_create")
+        self._h = h
+        self.shape = (self.m, self.pd.N[2], self.pd.N[1], self.pd.N[0])
+        self.size = int(L.rism3d_ctx_size(h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _abi.lib().rism3d_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def zeros(self, dtype=None):
+        t = self._torch
+        return t.zeros(self.shape, dtype=dtype or t.float64, device="cuda")
+
+    def _check_vec(self, x, dtype):
+        t = self._torch
+        if not (x.is_cuda and x.dtype == dtype and x.is_contiguous() and x.numel() == self.size):
+            raise ValueError(f"expected a contiguous CUDA {dtype} tensor of {self.size} elements")
+        if x.data_ptr() % 16:
+            raise ValueError("tensor must be 16-byte aligned")
+        return ctypes.c_void_p(x.data_ptr())
+
+    def iterate_t1(self, T, out=None):
+        """F(T) = (chi-1)*c(T) - beta/eps0 tau - T; returns (F, (|F|inf, |F|2))."""
+        t = self._torch
+        f32 = T.dtype == t.float32
+        out = t.empty_like(T) if out is None else out
+        r = (ctypes.c_double * 2)()
+        fn = _abi.lib().rism3d_iterate_t1_f32 if f32 else _abi.lib().rism3d_iterate_t1
+        _abi.check(fn(self._h, self._check_vec(T, T.dtype), self._check_vec(out, T.dtype), r), "iterate_t1")
+        return out, (r[0], r[1])
+
+    def jacobian_t1(self, T, dT, out=None):
+        """J(T) dT = (chi-1)*(c'(T) dT) - dT."""
+        t = self._torch
+        f32 = T.dtype == t.float32
+        out = t.empty_like(dT) if out is None else out
+        fn = _abi.lib().rism3d_jacobian_t1_f32 if f32 else _abi.lib().rism3d_jacobian_t1
+        _abi.check(fn(self._h, self._check_vec(T, T.dtype), self._check_vec(dT, T.dtype),
+                      self._check_vec(out, T.dtype)), "jacobian_t1")
+        return out
+
+    def solve(self, T=None):
+        """Newton solve in place on a device FP64 tensor; returns (T, result dict)."""
+        T = self.zeros() if T is None else T
+        res = _abi.Result()
+        rc = _abi.lib().rism3d_solve(self._h, self._check_vec(T, self._torch.float64), ctypes.byref(res))
+        if rc not in (_abi.OK, _abi.ERR_NOT_CONVERGED, _abi.ERR_NAN):
+            raise _abi.RismError(rc, "rism3d_solve")
+        return T, _result_dict(res)
+
+    def observables(self, T, want_g=False):
+        res = _abi.Result()
+        g = self.zeros() if want_g else None
+        _abi.check(_abi.lib().rism3d_observables(
+            self._h, self._check_vec(T, self._torch.float64),
+            self._check_vec(g, self._torch.float64) if g is not None else None,
+            ctypes.byref(res)), "rism3d_observables")
+        d = _result_dict(res)
+        d["GUV"] = g
+        return d
+
+    def field(self, which=0):
+        t = self._torch
+        out = self.zeros() if which == 0 else t.zeros(self.shape[1:], dtype=t.float64, device="cuda")
+        _abi.check(_abi.lib().rism3d_get_field(self._h, which, ctypes.c_void_p(out.data_ptr())), "get_field")
+        return out
+
+    def profile(self, on=True):
+        """Enable/disable per-pass event timing; returns the previous totals
+        {pass: (ms, launches)} for x-fwd, y, z, x-inv, vector ops."""
+        ms = (ctypes.c_double * 5)()
+        ln = (ctypes.c_longlong * 5)()
+        _abi.check(_abi.lib().rism3d_profile(self._h, 1 if on else 0, ms, ln), "profile")
+        names = ["xfwd", "y", "z", "xinv", "vec"]
+        return {k: (ms[i], ln[i]) for i, k in enumerate(names)}

@@ -1,0 +1,180 @@
+/*
+  rism3d.h -- C ABI of the B200-native 3D-RISM solute solver.
+
+  This is the drop-in boundary for the hot path of bgy3d's
+  ``runbgy.scm energy --hnc``: the hnc3d.c fixed-point / Newton loop.
+  Every entry point takes plain pointers and sizes; no PETSc, Guile or
+  torch types cross it.  All entry points return 0 on success and a
+  negative RISM3D_ERR_* code on failure (the reference longjmps through
+  scm_misc_error instead, bgy3d-snes.c:338-345).
+
+  Units are the reference's: Angstrom, kcal/mol, elementary charges,
+  beta in mol/kcal (bgy3d.h:120-145, units.f90).
+
+  Array layouts:
+    real grid field    [m][N2][N1][N0], N0 (x) fastest -- the DMDA order of
+                       bgy3d-fftw3.c:295-339; grid point (i0,i1,i2) sits at
+                       r = i*h - L/2 (vec_rmap3, bgy3d-vec.h:578-607).
+    solvent chi(k)     [m][m][nrad] on k_p = (p + 1/2) * pi / rmax -- the
+                       buffer rism_solvent() fills (rism.f90:57-102) and
+                       hnc3d_solute_solve() consumes (hnc3d.c:1442-1560).
+*/
+#ifndef RISM3D_H
+#define RISM3D_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Closures, numbered as ClosureEnum (bgy3d.h:211-223). */
+enum {
+  RISM3D_HNC = 0, RISM3D_KH = 1, RISM3D_PY = 2,
+  RISM3D_PSE0 = 3, RISM3D_PSE1, RISM3D_PSE2, RISM3D_PSE3,
+  RISM3D_PSE4, RISM3D_PSE5, RISM3D_PSE6, RISM3D_PSE7
+};
+
+/* Non-linear solvers, as --snes-solver (bgy3d-snes.c:16-35). */
+enum { RISM3D_NEWTON = 0, RISM3D_PICARD = 1, RISM3D_TRIAL = 2 };
+
+/* Arithmetic of the solve. */
+enum {
+  RISM3D_FP64 = 0,   /* plain form: every F, J.v and Krylov vector in FP64 */
+  RISM3D_MIXED = 1   /* FP32 bulk Newton, then FP64 residual + FP32 J.v
+                        iterative refinement to the same tolerance */
+};
+
+/* Status codes. */
+enum {
+  RISM3D_OK = 0,
+  RISM3D_ERR_ARG = -1,        /* bad argument (size, NULL, layout)        */
+  RISM3D_ERR_CUDA = -2,       /* CUDA runtime error                       */
+  RISM3D_ERR_NOMEM = -3,      /* device allocation failed                 */
+  RISM3D_ERR_TABLE = -4,      /* |k| of the grid beyond the chi table     */
+  RISM3D_ERR_NOT_CONVERGED = -5, /* max_iter reached (SNES reason <= 0)   */
+  RISM3D_ERR_NAN = -6,        /* residual became NaN/Inf                  */
+  RISM3D_ERR_UNSUPPORTED = -7 /* e.g. PY closure has no Jacobian          */
+};
+
+/* Mirrors ``Site`` (bgy3d-solutes.h:9-16) without the SCM handle. */
+typedef struct rism3d_site {
+  char name[8];
+  double x[3];        /* Angstrom */
+  double sigma;       /* LJ sigma, Angstrom */
+  double epsilon;     /* LJ epsilon, kcal/mol */
+  double charge;      /* e */
+} rism3d_site;
+
+/* Mirrors ``ProblemData`` (bgy3d.h:228-256) plus the flags the reference
+   reads through bgy3d_getopt_* (hnc3d.c:1782-1784, 1613-1627;
+   bgy3d-snes.c:20). */
+typedef struct rism3d_problem {
+  int N[3];           /* grid points; each 2^a 3^b, even, 8..512 */
+  double L[3];        /* FULL box edges (the reference's PD->L = 2 * --L,
+                         bgy3d-guile.c:284-288) */
+  double beta;        /* inverse temperature, mol/kcal */
+  double rho;         /* solvent site density, 1/A^3 */
+  double rmax;        /* radial extent of chi (1D grid), A */
+  int nrad;           /* radial points of chi */
+  int closure;        /* RISM3D_HNC ... RISM3D_PSE7 */
+  int max_iter;       /* Newton iterations (PD->max_iter) */
+  double norm_tol;    /* stop when ||F(t)||_inf < norm_tol */
+  double lambda;      /* Picard mixing (PD->lambda) */
+  int solver;         /* RISM3D_NEWTON / _PICARD / _TRIAL */
+  int renorm;         /* 1: default; 0: --no-renorm (hnc3d.c:1607-1615) */
+  int precision;      /* RISM3D_FP64 or RISM3D_MIXED */
+  int verbosity;      /* 0 silent; 1 one line per Newton step on stderr */
+} rism3d_problem;
+
+/* What hnc3d_solute_solve conses onto its result alist
+   (hnc3d.c:2230-2267) plus solver diagnostics. */
+typedef struct rism3d_result {
+  double mu;          /* free-energy: functional of the native closure */
+  double mu_hnc, mu_kh, mu_gf; /* print_chempot, hnc3d.c:668-687 */
+  double pmv_factor;  /* partial-molar-volume-factor, 1 - rho int c */
+  double resid_inf;   /* ||F(t)||_inf at exit (vec_norm, bgy3d-vec.h:301) */
+  double resid_2;     /* ||F(t)||_2 at exit (SNES norm) */
+  int status;         /* RISM3D_OK or RISM3D_ERR_* */
+  int newton_iters;
+  int f_evals;        /* F evaluations (iterate_t1), all precisions */
+  int jv_evals;       /* J.v products (jacobian_t1), all precisions */
+  int f_evals_fp32, jv_evals_fp32;
+  double seconds;     /* device time of the non-linear solve */
+} rism3d_result;
+
+/* Defaults of bgy3d-guile.c:243-386 / guile/bgy3d.scm:323-340 for a cubic
+   box: half edge ``L_half`` (the --L flag), N points per edge. */
+void rism3d_problem_defaults(rism3d_problem *pd, double L_half, int N);
+
+/*
+  One complete solute solve.  Replaces hnc3d_solute_solve()
+  (hnc3d.h:13-21, hnc3d.c:1762-2350) with the 1D-RISM chi supplied by the
+  caller (the chi_fft_buf != NULL branch, hnc3d.c:1449-1469).
+
+    chi      [m][m][nrad] solvent susceptibility chi = omega + rho h
+             (NOT offset by one), host memory, borrowed.
+    t_inout  host [m][N2][N1][N0] or NULL.  If non-NULL it is the initial
+             guess on entry and the converged t on exit -- the Restart
+             token of hnc3d.c:1830-1845, 2301-2316.
+    g_out    host [m][N2][N1][N0] or NULL: g = h + 1 (hnc3d.c:2320, 2341).
+    out      results; out->status repeats the return code.
+*/
+int rism3d_solute_solve(const rism3d_problem *pd,
+                        int m, const rism3d_site *solvent,
+                        int n, const rism3d_site *solute,
+                        const double *chi,
+                        double *t_inout, double *g_out,
+                        rism3d_result *out);
+
+/* ---- device-resident context: the inner plug points ------------------ */
+
+typedef struct rism3d_ctx rism3d_ctx;
+
+/* Builds everything hnc3d_solute_solve sets up before SNES
+   (hnc3d.c:1790-1966): the solute field v_short (bgy3d_solute_field /
+   field0, bgy3d-solutes.c:343-377, 845-969), chi - 1 and the renormalised
+   long-range kernel tau as radial tables (solvent_kernel_rism,
+   hnc3d.c:1442-1560; rism_solvent_renorm, rism.f90:141-208) and the
+   centred electric form factor (bgy3d_solute_form, bgy3d-solutes.c:633-698).
+   The context owns its device memory; it is bound to the current device. */
+int rism3d_ctx_create(const rism3d_problem *pd,
+                      int m, const rism3d_site *solvent,
+                      int n, const rism3d_site *solute,
+                      const double *chi, rism3d_ctx **ctx);
+void rism3d_ctx_destroy(rism3d_ctx *ctx);
+
+/* Number of reals in one long vector T: m * N0 * N1 * N2. */
+long long rism3d_ctx_size(const rism3d_ctx *ctx);
+
+/* F(T) = (chi-1) * c(T) - beta/eps0 tau - T: the VecFunc1 iterate_t1
+   (hnc3d.c:1183-1285).  T, dT: device pointers, FP64, [m][N2][N1][N0].
+   resid (optional, host, 2 doubles) receives ||dT||_inf and ||dT||_2. */
+int rism3d_iterate_t1(rism3d_ctx *ctx, const double *T, double *dT, double *resid);
+
+/* J(T) dT = (chi-1) * (c'(T) dT) - dT: the VecFunc2 jacobian_t1
+   (hnc3d.c:1289-1362).  Device pointers, FP64. */
+int rism3d_jacobian_t1(rism3d_ctx *ctx, const double *T, const double *dT, double *JdT);
+
+/* FP32 forms of the two above (device pointers to float). */
+int rism3d_iterate_t1_f32(rism3d_ctx *ctx, const float *T, float *dT, double *resid);
+int rism3d_jacobian_t1_f32(rism3d_ctx *ctx, const float *T, const float *dT, float *JdT);
+
+/* Solve F(T) = 0 in place (T on the device, FP64): the bgy3d_snes_default
+   call of hnc3d.c:1967 with the solver/precision of the problem. */
+int rism3d_solve(rism3d_ctx *ctx, double *T, rism3d_result *out);
+
+/* Post-processing of a converged T (hnc3d.c:2148-2269): mu by the native,
+   HNC, KH and GF functionals, PMV factor; g = h + 1 into g (device, FP64,
+   optional). */
+int rism3d_observables(rism3d_ctx *ctx, const double *T, double *g, rism3d_result *out);
+
+/* Copies an internal real field to a device buffer of [m][N] (which = 0:
+   v_short, 1: long-range Coulomb uc (one field, [N])). */
+int rism3d_get_field(rism3d_ctx *ctx, int which, double *dst);
+
+/* Last CUDA error string of this thread (diagnostics). */
+const char *rism3d_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RISM3D_H */
