@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""Benchmark: 3D-RISM solute solves per second to ||F(t)||_inf < 1e-10.
+
+Workload (one "step" = one complete solve from t = 0):
+  3D-RISM/KH, a 24-site synthetic neutral solute (seeded PCG64, sites in a
+  6 A ball, 1.2 A minimum separation, q ~ U[-0.8, 0.8] shifted to zero,
+  sigma ~ U[2.5, 4], eps ~ U[0.05, 0.3]) in PR-SPC/E water, chi from 1D
+  DRISM/KH (rmax 160 A, nrad 4096, eps_r 78.4), rho 0.0333295, beta 1.6889;
+  grid 256^3 with half edge L = 24 A (48 A box, h = 0.1875 A).
+  Synthetic data stand in for the reference's molecule inputs.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Our arm: mixed precision (FP32 bulk Newton, FP64 residual + FP32 Jacobian
+refinement); the plain FP64 form of the same solve is timed beside it.
+The reference arm (--impl reference) times the CPU restatement of the
+reference's algorithm (the reference itself cannot be built here) on a
+bounded sample of residual and Jacobian evaluations, scaled by the number
+of evaluations a full solve takes.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solves/s to ‖r‖<1e-10 @256³ 3D-RISM: mixed+batched vs plain FP64, 1 B200"
+GRID = 256
+N_SITES = 24
+SETTINGS = {"L": 24.0, "rho": 0.0333295, "beta": 1.6889, "closure": "KH", "rmax": 160.0, "nrad": 4096,
+            "norm-tol": 1e-10, "dielectric": 78.4, "max-iter": 200}
+# Residual (iterate_t1) and Jacobian (jacobian_t1) evaluations of one plain
+# FP64 Newton-GMRES solve of this workload -- the same algorithm the
+# reference drives through PETSc SNES -- used to scale the CPU samples.
+FP64_SOLVE_EVALS = {"f": 26, "jv": 76}
+
+
+def workload(grid=GRID):
+    from bgy3d_b200 import find_molecule, rism_solvent, synthetic_solute
+    solvent = find_molecule("water, PR-SPC/E")
+    solute = synthetic_solute(N_SITES, radius=6.0, seed=20261203)
+    s = dict(SETTINGS, N=grid)
+    chi = rism_solvent(solvent, dict(s, **{"norm-tol": 1e-12}))["susceptibility"]
+    return solute, solvent, s, chi
+
+
+def config(grid=GRID, precision="mixed"):
+    return {"workload": f"3D-RISM/KH solute solve to |F|inf<1e-10: {N_SITES}-site synthetic neutral solute "
+                        f"in PR-SPC/E water (3 sites), {grid}^3 grid, 48 A box, chi from 1D DRISM "
+                        f"(rmax 160, nrad 4096)", "grid": grid, "solute_sites": N_SITES, "solvent_sites": 3,
+            "closure": "KH", "tolerance": 1e-10, "precision": precision,
+            "l2": "fields of 67-201 MB per vector exceed the 126 MB L2; no flush needed"}
+
+
+def clocks_start():
+    f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    try:
+        p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                             stdout=f, stderr=subprocess.DEVNULL)
+    except OSError:
+        p = None
+    return p, f.name
+
+
+def clocks_stop(p, path, dev=0):
+    if p is None:
+        return None
+    p.terminate()
+    try:
+        p.wait(timeout=5)
+    except subprocess.TimeoutExpired:
+        p.kill()
+    sm, smax, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in open(path):
+        f = [x.strip() for x in line.split(",")]
+        if len(f) < 9 or not f[0].isdigit() or int(f[0]) != dev:
+            continue
+        try:
+            sm.append(float(f[1]))
+            smax = float(f[2])
+        except ValueError:
+            continue
+        for k, v in zip(names, f[5:9]):
+            if v.lower().startswith("active"):
+                reasons.add(k)
+    os.unlink(path)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(path))["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def pass_bytes(grid, m, b, launches, f_evals):
+    """Algorithmic HBM bytes of each pass over all its launches (b = bytes per real)."""
+    nr = grid ** 3
+    nc = (grid // 2 + 1) * grid * grid  # complex half-spectrum points per site
+    per = {
+        "xfwd": m * (2 * nr * b + nc * 2 * b),        # read t (or dt) and v (or d), write W
+        "y": m * 2 * nc * 2 * b,                      # read + write W
+        "z": m * 2 * nc * 2 * b,                      # read + write W (+ long-range field in F)
+        "xinv": m * (nc * 2 * b + 2 * nr * b),        # read W and t (or dt), write F
+    }
+    out = {k: per[k] * launches.get(k, 0) for k in per}
+    out["z"] += f_evals * nc * 2 * b
+    return out
+
+
+def run_ours(args, rank, world):
+    import torch
+    import torch.distributed as dist
+    from bgy3d_b200 import RismContext, hnc3d_run_solute
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    solute, solvent, s, chi = workload(args.grid)
+    ctx = RismContext(solute, solvent, dict(s, precision="mixed"), chi)
+    T = ctx.zeros()
+
+    def one(c):
+        T.zero_()
+        _, res = c.solve(T)
+        obs = c.observables(T)
+        return res, obs
+
+    for _ in range(args.warmup):
+        res, obs = one(ctx)
+    if res["status"] != 0:
+        raise RuntimeError(f"solve failed: {res}")
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ctx.profile(False)  # reset launch counters
+    clk, clk_path = clocks_start() if rank == 0 else (None, None)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(args.steps):
+        res, obs = one(ctx)
+    stop.record()
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(stop)
+    clocks = clocks_stop(clk, clk_path, dev) if rank == 0 else None
+    launches = sum(v[1] for v in ctx.profile(False).values())
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    mixed = {"res": res, "obs": obs}
+
+    # plain FP64 form of the same solve (the metric's comparison point)
+    ctx64 = RismContext(solute, solvent, dict(s, precision="fp64"), chi)
+    res64, obs64 = one(ctx64)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k64 = max(1, min(args.steps, 2))
+    e0.record()
+    for _ in range(k64):
+        res64, obs64 = one(ctx64)
+    e1.record()
+    torch.cuda.synchronize()
+    ms64 = e0.elapsed_time(e1) / k64
+
+    # per-pass device time of one mixed solve, for the roofline
+    ctx.profile(True)
+    one(ctx)
+    prof = ctx.profile(False)
+    ctx64.close()
+
+    # end to end through the host-buffer C-ABI call (hnc3d_run_solute)
+    torch.cuda.synchronize()
+    k_e2e = max(1, min(args.steps, 2))
+    t0 = time.perf_counter()
+    for _ in range(k_e2e):
+        out = hnc3d_run_solute(solute, solvent, dict(s, precision="mixed"), chi, want_g=True,
+                               want_restart=False)
+    e2e_s = (time.perf_counter() - t0) / k_e2e
+    ctx.close()
+    if rank != 0:
+        return None
+
+    m = 3
+    bw, src = hbm_peak()
+    best = None
+    for prec, b in (("f64", 8), ("f32", 4)):
+        lau = {k: prof[(k, prec)][1] for k in ("xfwd", "y", "z", "xinv")}
+        fe = res["f-evals"] if prec == "f64" else res["f-evals-fp32"]
+        byt = pass_bytes(args.grid, m, b, lau, fe)
+        for k in ("xfwd", "y", "z", "xinv"):
+            t_ms, n = prof[(k, prec)]
+            if n and (best is None or t_ms > best[2]):
+                best = (k, prec, t_ms, n, byt[k])
+    k, prec, t_ms, n, byt = best
+    achieved = byt / n / (t_ms / n * 1e-3) / 1e9
+    total_ms = sum(v[0] for v in prof.values())
+    value = world * args.steps / (ms * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64 (mixed)", "data": "synthetic (seeded solute, 1D-DRISM chi)",
+        "config": dict(config(args.grid), parallelism=f"replicas x{world} (independent solutes)"),
+        "fp64": {"value": 1e3 / ms64, "unit": "solves/s", "ms_per_step": ms64,
+                 "newton": res64["newton-iters"], "f_evals": res64["f-evals"], "jv_evals": res64["jv-evals"],
+                 "mu": obs64["free-energy"]},
+        "speedup_vs_fp64": ms64 / (ms / args.steps),
+        "solve": {"mu": mixed["obs"]["free-energy"], "mu_fp64": obs64["free-energy"],
+                  "dmu_vs_fp64": mixed["obs"]["free-energy"] - obs64["free-energy"],
+                  "resid_inf": res["resid-inf"], "newton": res["newton-iters"],
+                  "f_evals_f64": res["f-evals"], "jv_evals_f64": res["jv-evals"],
+                  "f_evals_f32": res["f-evals-fp32"], "jv_evals_f32": res["jv-evals-fp32"]},
+        "roofline": {"bound": "hbm", "kernel": f"{k} pass ({prec})", "achieved": achieved, "peak": bw,
+                     "peak_source": src, "unit": "GB/s", "frac": achieved / bw, "traffic": None,
+                     "bytes_per_launch": byt / n, "share_of_solve": t_ms / total_ms,
+                     "passes_ms": {f"{a}/{p}": round(v[0], 3) for (a, p), v in prof.items() if v[1]}},
+        "e2e": {"value": 1.0 / e2e_s, "unit": "solves/s",
+                "h2d_bytes_per_step": int(chi.nbytes + 2 * 64 * (N_SITES + 3)),
+                "d2h_bytes_per_step": int(out["GUV"].nbytes)},
+        "gpu_launches": int(launches),
+    }
+    if clocks:
+        line["clocks"] = clocks
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, sample_evals=1)
+    return line
+
+
+def cpu_sample(grid, sample_evals):
+    """Time sample_evals residual and Jacobian evaluations of the CPU
+    restatement at the full workload size; return seconds per solve."""
+    import os as _os
+    from oracle import hnc3d
+    from oracle import closures as cl
+    solute, solvent, s, chi = workload(grid)
+    P = hnc3d.Problem((grid,) * 3, (2 * s["L"],) * 3, s["beta"], s["rho"], cl.KH, solvent, solute, chi,
+                      s["rmax"])
+    T = np.zeros((3, grid, grid, grid))
+    P.iterate_t1(T)  # warm the FFT plans
+    t0 = time.perf_counter()
+    for _ in range(sample_evals):
+        F = P.iterate_t1(T)
+    tf = (time.perf_counter() - t0) / sample_evals
+    t0 = time.perf_counter()
+    for _ in range(sample_evals):
+        P.jacobian_t1(T, F)
+    tj = (time.perf_counter() - t0) / sample_evals
+    per_solve = FP64_SOLVE_EVALS["f"] * tf + FP64_SOLVE_EVALS["jv"] * tj
+    return per_solve, tf, tj, _os.cpu_count()
+
+
+def cpu_baseline(args, sample_evals=1):
+    per_solve, tf, tj, cores = cpu_sample(args.grid, sample_evals)
+    return {"value": 1.0 / per_solve, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": f"{sample_evals} iterate_t1 + {sample_evals} jacobian_t1 of the NumPy/SciPy restatement "
+                      f"at {args.grid}^3 ({tf:.2f} s + {tj:.2f} s), scaled by the {FP64_SOLVE_EVALS['f']} + "
+                      f"{FP64_SOLVE_EVALS['jv']} evaluations of one FP64 Newton-GMRES solve"}
+
+
+def run_reference(args):
+    times = []
+    for _ in range(args.warmup + args.steps):
+        per_solve, tf, tj, cores = cpu_sample(args.grid, 1)
+        times.append(per_solve)
+    t = times[args.warmup:]
+    value = len(t) / sum(t)
+    return {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sum(t) / len(t), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+            "data": "synthetic (seeded solute, 1D-DRISM chi)", "config": config(args.grid, "fp64"),
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
+                             "sample": "per step: one iterate_t1 + one jacobian_t1 of the NumPy/SciPy "
+                                       "restatement of hnc3d.c (the reference needs PETSc/FFTW/MPI/Guile, "
+                                       "absent here), scaled by the evaluations of one FP64 Newton solve"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--grid", type=int, default=GRID)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)))
+        return
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    line = run_ours(args, rank, world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -58,7 +58,7 @@ EXPORTS = [
     "rism3d_ctx_destroy", "rism3d_ctx_size", "rism3d_iterate_t1",
     "rism3d_jacobian_t1", "rism3d_iterate_t1_f32", "rism3d_jacobian_t1_f32",
     "rism3d_solve", "rism3d_observables", "rism3d_get_field", "rism3d_last_error",
-    "rism3d_profile",
+    "rism3d_profile", "rism1d_solvent_chi",
 ]
 
 _lib = None
@@ -99,6 +99,8 @@ def lib():
     L.rism3d_last_error.restype = ctypes.c_char_p
     L.rism3d_profile.argtypes = [V, I, P(D), P(ctypes.c_longlong)]
     L.rism3d_profile.restype = I
+    L.rism1d_solvent_chi.argtypes = [P(Problem), D, I, P(Site), P(D), P(D), P(D)]
+    L.rism1d_solvent_chi.restype = I
     _lib = L
     return L
 

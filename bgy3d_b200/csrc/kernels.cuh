@@ -356,8 +356,13 @@ __global__ void __launch_bounds__(256) k_xinv(Geo g, AxisPlan px, int RX,
     zk.x = zk.y = zm.x = zm.y = T(0);
     if (grow < rows_total) {
       const V *row_in = W + wbase + (long long)grow * g.Nhp;
-      const V xk = row_in[k];
-      const V xm = row_in[M - k];
+      V xk = row_in[k];
+      V xm = row_in[M - k];
+      // The 1D c2r stage reads only the real parts of the kx = 0 and
+      // kx = N0/2 elements (as FFTW / pocketfft do).  They are real for a
+      // Hermitian spectrum; the long-range term is not Hermitian on the ky /
+      // kz Nyquist planes, which leaves imaginary parts here.
+      if (k == 0) { xk.y = T(0); xm.y = T(0); }
       // A = X_k + conj X_{M-k}, D = X_k - conj X_{M-k}, P = D conj(w_k)
       V Aa, D;
       Aa.x = xk.x + xm.x; Aa.y = xk.y - xm.y;

@@ -114,8 +114,8 @@ struct TileShape {
 struct PassTimer {
   bool on = false;
   cudaEvent_t a, b;
-  double ms[8] = {0};
-  long long launches[8] = {0};
+  double ms[10] = {0};
+  long long launches[10] = {0};
 };
 
 struct rism3d_ctx {
@@ -188,10 +188,13 @@ namespace {
 
 enum { TK_XFWD = 0, TK_Y = 1, TK_Z = 2, TK_XINV = 3, TK_VEC = 4 };
 
+// Times one pass (when enabled) into bucket which + 5 * precision and
+// always counts its kernel launches.
 struct TimeScope {
   rism3d_ctx *c;
   int which;
-  TimeScope(rism3d_ctx *c_, int w) : c(c_), which(w) {
+  TimeScope(rism3d_ctx *c_, int w, int prec, int nlaunch = 1) : c(c_), which(w + 5 * prec) {
+    c->timer.launches[which] += nlaunch;
     if (c->timer.on) cudaEventRecord(c->timer.a, c->stream);
   }
   ~TimeScope() {
@@ -201,7 +204,6 @@ struct TimeScope {
       float ms = 0;
       cudaEventElapsedTime(&ms, c->timer.a, c->timer.b);
       c->timer.ms[which] += ms;
-      c->timer.launches[which] += 1;
     }
   }
 };
@@ -252,7 +254,7 @@ template <typename T> size_t zsmem(rism3d_ctx *c) {
 }
 
 template <typename T, bool INV> void launch_y(rism3d_ctx *c) {
-  TimeScope ts(c, TK_Y);
+  TimeScope ts(c, TK_Y, sizeof(T) == 8 ? 0 : 1);
   dim3 grid((c->g.Nh + c->tl<T>().BY - 1) / c->tl<T>().BY, c->g.N2, c->m);
   const size_t sm = ysmem<T>(c);
   auto *W = c->work<T>();
@@ -263,7 +265,7 @@ template <typename T, bool INV> void launch_y(rism3d_ctx *c) {
 }
 
 template <typename T, int MODE> void launch_z(rism3d_ctx *c) {
-  TimeScope ts(c, TK_Z);
+  TimeScope ts(c, TK_Z, sizeof(T) == 8 ? 0 : 1);
   dim3 grid((c->g.Nh + c->tl<T>().BZ - 1) / c->tl<T>().BZ, c->g.N1);
   const size_t sm = zsmem<T>(c);
   auto *W = c->work<T>();
@@ -295,7 +297,7 @@ template <typename T> void eval_F(rism3d_ctx *c, const T *x, T *out, double *res
   dim3 gx((rows + c->tl<T>().RX - 1) / c->tl<T>().RX, c->m);
   auto *W = c->work<T>();
   {
-    TimeScope ts(c, TK_XFWD);
+    TimeScope ts(c, TK_XFWD, sizeof(T) == 8 ? 0 : 1);
     k_xfwd<T, MODE_F><<<gx, 256, xsmem<T>(c), c->stream>>>(c->g, c->plan<T>(0), c->tl<T>().RX, x, vfield<T>(c),
                                                           (T)c->pd.beta, c->pd.closure, W, postw<T>(c));
     CKL();
@@ -304,7 +306,7 @@ template <typename T> void eval_F(rism3d_ctx *c, const T *x, T *out, double *res
   launch_z<T, MODE_F>(c);
   launch_y<T, true>(c);
   {
-    TimeScope ts(c, TK_XINV);
+    TimeScope ts(c, TK_XINV, sizeof(T) == 8 ? 0 : 1);
     k_xinv<T><<<gx, 256, xsmem<T>(c), c->stream>>>(c->g, c->plan<T>(0), c->tl<T>().RX, W, x, out,
                                                    (T)(1.0 / (double)c->g.Nr), (T)1, postw<T>(c), c->npart);
     CKL();
@@ -319,7 +321,7 @@ template <typename T> void eval_J(rism3d_ctx *c, const T *d, const T *vin, doubl
   dim3 gx((rows + c->tl<T>().RX - 1) / c->tl<T>().RX, c->m);
   auto *W = c->work<T>();
   {
-    TimeScope ts(c, TK_XFWD);
+    TimeScope ts(c, TK_XFWD, sizeof(T) == 8 ? 0 : 1);
     k_xfwd<T, MODE_J><<<gx, 256, xsmem<T>(c), c->stream>>>(c->g, c->plan<T>(0), c->tl<T>().RX, vin, d, (T)s,
                                                           c->pd.closure, W, postw<T>(c));
     CKL();
@@ -328,7 +330,7 @@ template <typename T> void eval_J(rism3d_ctx *c, const T *d, const T *vin, doubl
   launch_z<T, MODE_J>(c);
   launch_y<T, true>(c);
   {
-    TimeScope ts(c, TK_XINV);
+    TimeScope ts(c, TK_XINV, sizeof(T) == 8 ? 0 : 1);
     k_xinv<T><<<gx, 256, xsmem<T>(c), c->stream>>>(c->g, c->plan<T>(0), c->tl<T>().RX, W, vin, out,
                                                    (T)(1.0 / (double)c->g.Nr), (T)s, postw<T>(c), c->npart);
     CKL();
@@ -347,7 +349,7 @@ template <typename T> VecRef<T> vref(const T *p, double s) { return VecRef<T>{p,
 // h[i] = <w * ws, s_i V_i> for i < nv.
 template <typename T>
 void mdot(rism3d_ctx *c, const T *w, double ws, const std::vector<VecRef<T>> &V, std::vector<double> &h) {
-  TimeScope ts(c, TK_VEC);
+  TimeScope ts(c, TK_VEC, sizeof(T) == 8 ? 0 : 1, ((int)V.size() + kDotChunk - 1) / kDotChunk);
   const int nv = (int)V.size();
   h.assign(nv, 0.0);
   const int G = c->red_blocks;
@@ -371,7 +373,7 @@ void mdot(rism3d_ctx *c, const T *w, double ws, const std::vector<VecRef<T>> &V,
 template <typename T>
 double maxpy(rism3d_ctx *c, T *w, double ws, const std::vector<VecRef<T>> &V, const std::vector<double> &coef,
              bool want_norm) {
-  TimeScope ts(c, TK_VEC);
+  TimeScope ts(c, TK_VEC, sizeof(T) == 8 ? 0 : 1, std::max(1, ((int)V.size() + kDotChunk - 1) / kDotChunk));
   const int nv = (int)V.size();
   const int G = c->red_blocks;
   double *dcoef = c->dpart + (size_t)G * kDotChunk;  // scratch after the partials
@@ -406,13 +408,13 @@ double maxpy(rism3d_ctx *c, T *w, double ws, const std::vector<VecRef<T>> &V, co
 }
 
 template <typename TX, typename TY> void axpby(rism3d_ctx *c, double a, const TX *x, double b, TY *y) {
-  TimeScope ts(c, TK_VEC);
+  TimeScope ts(c, TK_VEC, sizeof(TY) == 8 ? 0 : 1);
   k_axpby<TX, TY><<<vec_grid(c->nvec), 256, 0, c->stream>>>(c->nvec, a, x, b, y);
   CKL();
 }
 template <typename TX, typename TY, typename TZ>
 void xpay(rism3d_ctx *c, const TX *x, double a, const TY *y, TZ *z) {
-  TimeScope ts(c, TK_VEC);
+  TimeScope ts(c, TK_VEC, sizeof(TZ) == 8 ? 0 : 1);
   k_xpay<TX, TY, TZ><<<vec_grid(c->nvec), 256, 0, c->stream>>>(c->nvec, x, a, y, z);
   CKL();
 }
@@ -532,7 +534,7 @@ template <typename TS> __global__ void k_slope_any(long long n, const TS *__rest
 }
 
 template <typename TS, typename TJ> void closure_slope(rism3d_ctx *c, const TS *x, TJ *d) {
-  TimeScope ts(c, TK_VEC);
+  TimeScope ts(c, TK_VEC, sizeof(TJ) == 8 ? 0 : 1);
   const long long n = c->nvec;
   float *d32 = sizeof(TJ) == 4 ? reinterpret_cast<float *>(d) : nullptr;
   double *d64 = sizeof(TJ) == 8 ? reinterpret_cast<double *>(d) : nullptr;
@@ -870,30 +872,41 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
     const int rows = G.N1 * G.N2;
     const int rxmin = std::min(c->tiles[0].RX, c->tiles[1].RX);
     c->npart = dalloc<NormPartial>((size_t)((rows + rxmin - 1) / rxmin) * m);
-    // shared-memory opt-in
-    const size_t sx64 = xsmem<double>(c), sy64 = ysmem<double>(c), sz64 = zsmem<double>(c);
-    const int big = 227 * 1024;
-    if (sx64 > (size_t)big || sy64 > (size_t)big || sz64 > (size_t)big)
-      throw ArgFail{RISM3D_ERR_ARG, "tile exceeds shared memory"};
-    CK(cudaFuncSetAttribute(k_xfwd<double, MODE_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_xfwd<double, MODE_J>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_xfwd<float, MODE_F>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_xfwd<float, MODE_J>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_xinv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    CK(cudaFuncSetAttribute(k_xinv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-#define OPTIN_YZ(T)                                                                                    \
-  CK(cudaFuncSetAttribute(k_y<T, false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));   \
-  CK(cudaFuncSetAttribute(k_y<T, true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));    \
-  CK(cudaFuncSetAttribute(k_y<T, false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));    \
-  CK(cudaFuncSetAttribute(k_y<T, true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));     \
-  CK(cudaFuncSetAttribute(k_y<T, false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));    \
-  CK(cudaFuncSetAttribute(k_y<T, true, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));     \
-  CK(cudaFuncSetAttribute(k_z<T, MODE_F, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));  \
-  CK(cudaFuncSetAttribute(k_z<T, MODE_J, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));  \
-  CK(cudaFuncSetAttribute(k_z<T, MODE_F, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));   \
-  CK(cudaFuncSetAttribute(k_z<T, MODE_J, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));   \
-  CK(cudaFuncSetAttribute(k_z<T, MODE_F, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));   \
-  CK(cudaFuncSetAttribute(k_z<T, MODE_J, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    // shared-memory opt-in: each kernel may use the device's per-block
+    // opt-in limit minus its own static shared memory
+    int dev = 0, optin = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    size_t need = 0;
+    for (size_t b : {xsmem<double>(c), ysmem<double>(c), zsmem<double>(c), xsmem<float>(c), ysmem<float>(c),
+                     zsmem<float>(c)})
+      need = std::max(need, b);
+    auto allow = [&](const void *fn) {
+      cudaFuncAttributes fa{};
+      CK(cudaFuncGetAttributes(&fa, fn));
+      const int dyn = optin - (int)fa.sharedSizeBytes;
+      if ((size_t)dyn < need) throw ArgFail{RISM3D_ERR_ARG, "tile exceeds shared memory"};
+      CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+    };
+    allow((const void *)k_xfwd<double, MODE_F>);
+    allow((const void *)k_xfwd<double, MODE_J>);
+    allow((const void *)k_xfwd<float, MODE_F>);
+    allow((const void *)k_xfwd<float, MODE_J>);
+    allow((const void *)k_xinv<double>);
+    allow((const void *)k_xinv<float>);
+#define OPTIN_YZ(T)                                  \
+  allow((const void *)k_y<T, false, 16>);            \
+  allow((const void *)k_y<T, true, 16>);             \
+  allow((const void *)k_y<T, false, 8>);             \
+  allow((const void *)k_y<T, true, 8>);              \
+  allow((const void *)k_y<T, false, 4>);             \
+  allow((const void *)k_y<T, true, 4>);              \
+  allow((const void *)k_z<T, MODE_F, 16>);           \
+  allow((const void *)k_z<T, MODE_J, 16>);           \
+  allow((const void *)k_z<T, MODE_F, 8>);            \
+  allow((const void *)k_z<T, MODE_J, 8>);            \
+  allow((const void *)k_z<T, MODE_F, 4>);            \
+  allow((const void *)k_z<T, MODE_J, 4>);
     OPTIN_YZ(double)
     OPTIN_YZ(float)
 #undef OPTIN_YZ
@@ -1064,9 +1077,9 @@ int rism3d_profile(rism3d_ctx *ctx, int on, double *ms_out, long long *launches_
   if (!ctx) return RISM3D_ERR_ARG;
   return guard([&] {
     if (ms_out)
-      for (int i = 0; i < 5; ++i) ms_out[i] = ctx->timer.ms[i];
+      for (int i = 0; i < 10; ++i) ms_out[i] = ctx->timer.ms[i];
     if (launches_out)
-      for (int i = 0; i < 5; ++i) launches_out[i] = ctx->timer.launches[i];
+      for (int i = 0; i < 10; ++i) launches_out[i] = ctx->timer.launches[i];
     if (on && !ctx->timer.on) {
       CK(cudaEventCreate(&ctx->timer.a));
       CK(cudaEventCreate(&ctx->timer.b));
@@ -1076,7 +1089,7 @@ int rism3d_profile(rism3d_ctx *ctx, int on, double *ms_out, long long *launches_
       cudaEventDestroy(ctx->timer.b);
       ctx->timer.on = false;
     }
-    for (int i = 0; i < 8; ++i) ctx->timer.ms[i] = 0, ctx->timer.launches[i] = 0;
+    for (int i = 0; i < 10; ++i) ctx->timer.ms[i] = 0, ctx->timer.launches[i] = 0;
     return (int)RISM3D_OK;
   });
 }

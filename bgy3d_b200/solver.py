@@ -84,12 +84,34 @@ def _result_dict(r):
     }
 
 
-def hnc3d_run_solute(solute, solvent, settings, chi, restart=None, want_g=True):
+def rism_solvent(solvent, settings):
+    """1D RISM/DRISM pure-solvent solve (rism1d_solvent_chi), mirroring the
+    Scheme ``rism-solvent`` (guile/bgy3d.scm:358-360 -> rism.f90:57-102).
+
+    Returns {"susceptibility": chi [m][m][nrad], "t": t(r), "free-energy": mu}.
+    The DRISM correction is applied when settings["dielectric"] != 0.  The
+    residual of r t(r) is driven below max(norm-tol, 1e-12)."""
+    L = _abi.lib()
+    pd = problem_data(settings)
+    pd.norm_tol = max(pd.norm_tol, 1e-12)
+    pd.max_iter = min(pd.max_iter, 500)
+    m = len(solvent)
+    chi = np.zeros((m, m, pd.nrad))
+    t = np.zeros((m, m, pd.nrad))
+    mu = ctypes.c_double()
+    rc = L.rism1d_solvent_chi(ctypes.byref(pd), float((settings or {}).get("dielectric", 0.0)), m,
+                              _sites(solvent), _dptr(chi), _dptr(t), ctypes.byref(mu))
+    _abi.check(rc, "rism_solvent")
+    return {"susceptibility": chi, "t": t, "free-energy": mu.value}
+
+
+def hnc3d_run_solute(solute, solvent, settings, chi, restart=None, want_g=True, want_restart=True):
     """One 3D-RISM solute solve with host buffers (rism3d_solute_solve).
 
     chi: [m][m][nrad] solvent susceptibility (not offset by one) on the
     radial k-grid (p + 1/2) pi / rmax; settings must then carry the rmax and
     nrad it was computed with.  restart: initial t [m][N2][N1][N0] or None.
+    With restart None and want_restart False no t crosses the host link.
     """
     L = _abi.lib()
     pd = problem_data(settings)
@@ -98,13 +120,17 @@ def hnc3d_run_solute(solute, solvent, settings, chi, restart=None, want_g=True):
     if chi.shape != (m, m, pd.nrad):
         raise ValueError(f"chi must be [{m}][{m}][{pd.nrad}], got {chi.shape}")
     shape = (m, pd.N[2], pd.N[1], pd.N[0])
-    t = np.zeros(shape) if restart is None else np.array(restart, dtype=np.float64, order="C", copy=True)
-    if t.shape != shape:
-        raise ValueError("restart has the wrong shape")
+    if restart is None and not want_restart:
+        t = None
+    else:
+        t = np.zeros(shape) if restart is None else np.array(restart, dtype=np.float64, order="C", copy=True)
+        if t.shape != shape:
+            raise ValueError("restart has the wrong shape")
     g = np.empty(shape) if want_g else None
     res = _abi.Result()
     rc = L.rism3d_solute_solve(ctypes.byref(pd), m, _sites(solvent), n, _sites(solute), _dptr(chi),
-                               _dptr(t), _dptr(g) if g is not None else None, ctypes.byref(res))
+                               _dptr(t) if t is not None else None, _dptr(g) if g is not None else None,
+                               ctypes.byref(res))
     out = _result_dict(res)
     if rc != _abi.OK and rc != _abi.ERR_NOT_CONVERGED:
         raise _abi.RismError(rc, "hnc3d_run_solute")
@@ -205,10 +231,12 @@ class RismContext:
         return out
 
     def profile(self, on=True):
-        """Enable/disable per-pass event timing; returns the previous totals
-        {pass: (ms, launches)} for x-fwd, y, z, x-inv, vector ops."""
-        ms = (ctypes.c_double * 5)()
-        ln = (ctypes.c_longlong * 5)()
+        """Enable/disable per-pass event timing; returns and resets the totals
+        {(pass, precision): (ms, launches)}, pass in xfwd/y/z/xinv/vec and
+        precision in f64/f32 (launches are counted with timing off too)."""
+        ms = (ctypes.c_double * 10)()
+        ln = (ctypes.c_longlong * 10)()
         _abi.check(_abi.lib().rism3d_profile(self._h, 1 if on else 0, ms, ln), "profile")
         names = ["xfwd", "y", "z", "xinv", "vec"]
-        return {k: (ms[i], ln[i]) for i, k in enumerate(names)}
+        return {(k, p): (ms[i + 5 * j], ln[i + 5 * j]) for j, p in enumerate(("f64", "f32"))
+                for i, k in enumerate(names)}

@@ -174,6 +174,29 @@ int rism3d_get_field(rism3d_ctx *ctx, int which, double *dst);
 /* Last CUDA error string of this thread (diagnostics). */
 const char *rism3d_last_error(void);
 
+/* Per-pass CUDA-event timing (diagnostics): on != 0 enables it (it
+   synchronises after every pass, so it is for measurement only).  The
+   totals accumulated since the last call are returned in ms[10] /
+   launches[10] (either may be NULL) and reset; bucket = pass + 5 * p with
+   pass 0..4 = x-forward, y, z, x-inverse, vector ops and p = 0 for FP64,
+   1 for FP32.  Launches are counted even when timing is off. */
+int rism3d_profile(rism3d_ctx *ctx, int on, double *ms, long long *launches);
+
+/* ---- solvent susceptibility (setup, CPU) ------------------------------ */
+
+/* 1D RISM / DRISM of the pure solvent: replaces rism_solvent()
+   (rism.f90:57-102, rism_vv 310-583).  Uses pd->beta, rho, rmax, nrad
+   (2^a 3^b), closure, norm_tol (on r t(r)) and max_iter.
+     dielectric  target epsilon of the DRISM correction (--dielectric), or 0
+                 for plain RISM;
+     chi         out, [m][m][nrad]: chi = omega + rho h -- the chi_fft_buf of
+                 hnc3d_solute_solve and of rism3d_solute_solve above;
+     t           optional, [m][m][nrad]: initial guess on entry, t(r) on exit;
+     mu          optional, out: the solvent's excess chemical potential. */
+int rism1d_solvent_chi(const rism3d_problem *pd, double dielectric, int m,
+                       const rism3d_site *solvent, double *chi, double *t,
+                       double *mu);
+
 #ifdef __cplusplus
 }
 #endif
