@@ -291,6 +291,37 @@ def run_reference(args):
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_evals(args):
+    """Profiling mode: args.evals residual and Jacobian evaluations in each
+    precision on the workload (no Newton solve); prints per-evaluation times."""
+    import torch
+    from bgy3d_b200 import RismContext
+    solute, solvent, s, chi = workload(args.grid)
+    ctx = RismContext(solute, solvent, s, chi)
+    out = {"grid": args.grid}
+    for dt in (torch.float32, torch.float64):
+        T = ctx.zeros(dt)
+        F, _ = ctx.iterate_t1(T)
+        ctx.jacobian_t1(T, F)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.evals):
+            ctx.iterate_t1(T, out=F)
+        e1.record()
+        torch.cuda.synchronize()
+        tf = e0.elapsed_time(e1) / args.evals
+        J = torch.empty_like(F)
+        e0.record()
+        for _ in range(args.evals):
+            ctx.jacobian_t1(T, F, out=J)
+        e1.record()
+        torch.cuda.synchronize()
+        out[str(dt).split(".")[-1]] = {"F_ms": tf, "Jv_ms": e0.elapsed_time(e1) / args.evals}
+    ctx.close()
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -299,7 +330,12 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--grid", type=int, default=GRID)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--evals", type=int, default=0,
+                    help="profiling mode: time this many F and J.v evaluations instead of solves")
     args = ap.parse_args()
+    if args.evals:
+        run_evals(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
