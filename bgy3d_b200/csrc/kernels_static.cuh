@@ -1,0 +1,302 @@
+// kernels_static.cuh -- shape-specialised FFT passes of the 3D-RISM residual
+// (the same five passes as kernels.cuh, for compile-time transform lengths).
+//
+//   k_xfwd_s  closure (or its linearisation) + r2c along x: RX contiguous rows
+//             per CTA, vector loads, padded shared-memory rows;
+//   k_y_s     one [N1][B] column tile per CTA, loaded and stored by TMA;
+//   k_z_s     the m [N2][B] tiles of one (ky, kx-block), TMA in and out, with
+//             the OZ contraction between the forward and inverse transforms;
+//   k_xinv_s  c2r along x with "- t" and the residual norms.
+//
+// B columns of a y/z tile are 128 bytes (16 float2 or 8 double2): one TMA box
+// row per transform index, so every HBM access is a whole 128-byte line.
+#pragma once
+#include "fft_static.cuh"
+#include "kernels.cuh"
+
+namespace rism {
+
+constexpr uint32_t kMbarPolls = 1u << 26;  // bounded mbarrier wait (seconds)
+
+template <typename T> struct VecW;  // complex values per vector load in the x passes
+template <> struct VecW<float> { static constexpr int n = 2; using vec = float4; };
+template <> struct VecW<double> { static constexpr int n = 1; using vec = double2; };
+
+// x forward (see k_xfwd): MODE_F c = closure(p B, A); MODE_J c = B (p A).
+template <typename T, int MODE, int M, int RX>
+__global__ void __launch_bounds__(256) k_xfwd_s(Geo g, const T *__restrict__ A, const T *__restrict__ Bv, T p,
+                                               int closure, typename Cx<T>::type *__restrict__ W,
+                                               const typename Cx<T>::type *__restrict__ post,
+                                               const typename Cx<T>::type *__restrict__ twg) {
+  using V = typename Cx<T>::type;
+  using Lay = LayRow<M, Split<M>::R2>;
+  constexpr int VW = VecW<T>::n;
+  using VEC = typename VecW<T>::vec;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V *tw = reinterpret_cast<V *>(smem_raw);
+  V *buf = tw + M;
+  const int tid = threadIdx.x;
+  const int rows_total = g.N1 * g.N2;
+  const int row0 = blockIdx.x * RX;
+  const int site = blockIdx.y;
+  for (int q = tid; q < M; q += 256) tw[q] = twg[q];
+  const long long sbase = (long long)site * g.Nr;
+  constexpr int PER_ROW = M / VW;
+#pragma unroll 4
+  for (int e = tid; e < RX * PER_ROW; e += 256) {
+    const int row = e / PER_ROW, jj = (e % PER_ROW) * VW;
+    const int grow = row0 + row;
+    V z[VW];
+#pragma unroll
+    for (int v = 0; v < VW; ++v) z[v].x = z[v].y = T(0);
+    if (grow < rows_total) {
+      const long long off = sbase + (long long)grow * g.N0 + 2 * jj;
+      const VEC a = *reinterpret_cast<const VEC *>(A + off);
+      const VEC b = *reinterpret_cast<const VEC *>(Bv + off);
+      const T *ar = reinterpret_cast<const T *>(&a);
+      const T *br = reinterpret_cast<const T *>(&b);
+#pragma unroll
+      for (int v = 0; v < VW; ++v) {
+        if (MODE == MODE_F) {
+          z[v].x = closure_c<T>(closure, p * br[2 * v], ar[2 * v]);
+          z[v].y = closure_c<T>(closure, p * br[2 * v + 1], ar[2 * v + 1]);
+        } else {
+          z[v].x = br[2 * v] * (ar[2 * v] * p);
+          z[v].y = br[2 * v + 1] * (ar[2 * v + 1] * p);
+        }
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < VW; ++v) buf[Lay::at(jj + v, row)] = z[v];
+  }
+  __syncthreads();
+  fft2<M, RX, 256, false, false, Lay>(buf, tw);
+  constexpr int H = M / 2 + 1;
+  const long long wbase = (long long)site * g.Nc;
+  for (int e = tid; e < RX * H; e += 256) {
+    const int row = e / H, k = e % H;
+    const int grow = row0 + row;
+    if (grow >= rows_total) continue;
+    const V zk = buf[Lay::at(k, row)];
+    const V zm = buf[Lay::at(k == 0 ? 0 : M - k, row)];
+    V E, O;
+    E.x = (zk.x + zm.x) * T(0.5);
+    E.y = (zk.y - zm.y) * T(0.5);
+    O.x = (zk.y + zm.y) * T(0.5);
+    O.y = -(zk.x - zm.x) * T(0.5);
+    const V wO = cmul(post[k], O);
+    V *row_out = W + wbase + (long long)grow * g.Nhp;
+    row_out[k] = cadd(E, wO);
+    if (M - k != k) row_out[M - k] = cconj(csub(E, wO));
+  }
+}
+
+// x inverse (see k_xinv): out = scale x - sub In, residual norms.
+template <typename T, int M, int RX>
+__global__ void __launch_bounds__(256) k_xinv_s(Geo g, const typename Cx<T>::type *__restrict__ W,
+                                               const T *__restrict__ In, T *__restrict__ Out, T scale, T sub,
+                                               const typename Cx<T>::type *__restrict__ post,
+                                               const typename Cx<T>::type *__restrict__ twg,
+                                               NormPartial *__restrict__ part) {
+  using V = typename Cx<T>::type;
+  using Lay = LayRow<M, Split<M>::R2>;
+  constexpr int VW = VecW<T>::n;
+  using VEC = typename VecW<T>::vec;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V *tw = reinterpret_cast<V *>(smem_raw);
+  V *buf = tw + M;
+  const int tid = threadIdx.x;
+  const int rows_total = g.N1 * g.N2;
+  const int row0 = blockIdx.x * RX;
+  const int site = blockIdx.y;
+  for (int q = tid; q < M; q += 256) tw[q] = twg[q];
+  constexpr int H = M / 2 + 1;
+  const long long wbase = (long long)site * g.Nc;
+#pragma unroll 2
+  for (int e = tid; e < RX * H; e += 256) {
+    const int row = e / H, k = e % H;
+    const int grow = row0 + row;
+    V zk, zm;
+    zk.x = zk.y = zm.x = zm.y = T(0);
+    if (grow < rows_total) {
+      const V *row_in = W + wbase + (long long)grow * g.Nhp;
+      V xk = row_in[k];
+      V xm = row_in[M - k];
+      if (k == 0) { xk.y = T(0); xm.y = T(0); }  // c2r reads only Re X_0, Re X_{N0/2}
+      V Aa, D;
+      Aa.x = xk.x + xm.x; Aa.y = xk.y - xm.y;
+      D.x = xk.x - xm.x;  D.y = xk.y + xm.y;
+      const V Pp = cmul(D, cconj(post[k]));
+      zk.x = Aa.x - Pp.y; zk.y = Aa.y + Pp.x;
+      zm.x = Aa.x + Pp.y; zm.y = -(Aa.y - Pp.x);
+    }
+    buf[Lay::at(k, row)] = zk;
+    if (k != 0 && M - k != k) buf[Lay::at(M - k, row)] = zm;
+  }
+  __syncthreads();
+  fft2<M, RX, 256, true, false, Lay>(buf, tw);
+  double amax = 0.0, sum2 = 0.0;
+  const long long sbase = (long long)site * g.Nr;
+  constexpr int PER_ROW = M / VW;
+#pragma unroll 4
+  for (int e = tid; e < RX * PER_ROW; e += 256) {
+    const int row = e / PER_ROW, jj = (e % PER_ROW) * VW;
+    const int grow = row0 + row;
+    if (grow >= rows_total) continue;
+    const long long off = sbase + (long long)grow * g.N0 + 2 * jj;
+    const VEC in = *reinterpret_cast<const VEC *>(In + off);
+    const T *ir = reinterpret_cast<const T *>(&in);
+    VEC o;
+    T *orr = reinterpret_cast<T *>(&o);
+#pragma unroll
+    for (int v = 0; v < VW; ++v) {
+      const V z = buf[Lay::at(jj + v, row)];
+      orr[2 * v] = z.x * scale - sub * ir[2 * v];
+      orr[2 * v + 1] = z.y * scale - sub * ir[2 * v + 1];
+    }
+    *reinterpret_cast<VEC *>(Out + off) = o;
+#pragma unroll
+    for (int v = 0; v < 2 * VW; ++v) {
+      const double ov = (double)orr[v];
+      amax = fmax(amax, fabs(ov));
+      sum2 += ov * ov;
+    }
+  }
+  block_norms(amax, sum2, part + (blockIdx.y * gridDim.x + blockIdx.x));
+}
+
+// y pass: one [N][B] tile (kx0 .. kx0+B-1 at fixed z, site) by TMA.
+// tm: W as {2 Nhp, N1, m N2} scalars, box {2B, N1, 1}.
+template <typename T, bool INV, int N, int B>
+__global__ void __launch_bounds__(Split<N>::R1 * B) k_y_s(Geo g, const __grid_constant__ CUtensorMap tm,
+                                                         const typename Cx<T>::type *__restrict__ twg,
+                                                         int *__restrict__ err) {
+  using V = typename Cx<T>::type;
+  constexpr int NTHR = Split<N>::R1 * B;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  V *buf = reinterpret_cast<V *>(smem_raw);
+  V *tw = buf + N * B;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(tw + N);
+  const int tid = threadIdx.x;
+  const int kx0 = blockIdx.x * B, z = blockIdx.y, site = blockIdx.z;
+  if (tid == 0) mbar_init(bar, 1);
+  __syncthreads();
+  if (tid == 0) {
+    mbar_expect_tx(bar, (uint32_t)(N * B * sizeof(V)));
+    tma_load_3d(buf, &tm, bar, 2 * kx0, 0, site * g.N2 + z);
+  }
+  for (int q = tid; q < N; q += NTHR) tw[q] = twg[q];
+  if (!mbar_wait(bar, 0, kMbarPolls)) {
+    if (tid == 0) atomicExch(err, 1);
+    return;
+  }
+  __syncthreads();
+  fft2<N, B, NTHR, INV, true, LayCol<N, B>>(buf, tw);
+  fence_proxy_async();
+  __syncthreads();
+  if (tid == 0) {
+    tma_store_3d(&tm, buf, 2 * kx0, 0, site * g.N2 + z);
+    tma_commit();
+    tma_wait_read0();
+  }
+}
+
+// z pass: the m [N][B] tiles of one (ky, kx-block) by TMA, forward transform,
+// OZ contraction (+ long-range terms in MODE_F), inverse transform, TMA out.
+// tm: W as {2 Nhp, N1, m N2} scalars, box {2B, 1, N2}.
+template <typename T, int MODE, int N, int B, int MS>
+__global__ void __launch_bounds__(Split<N>::R1 * B) k_z_s(Geo g, const __grid_constant__ CUtensorMap tm,
+                                                         const typename Cx<T>::type *__restrict__ twg,
+                                                         ZParams<T> zp, int *__restrict__ err) {
+  using V = typename Cx<T>::type;
+  using P2 = typename Vec2<T>::type;
+  constexpr int NTHR = Split<N>::R1 * B;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int m = g.m;
+  V *buf = reinterpret_cast<V *>(smem_raw);
+  V *tw = buf + m * N * B;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(tw + N);
+  const int tid = threadIdx.x;
+  const int kx0 = blockIdx.x * B, y = blockIdx.y;
+  const int bw = min(B, g.Nh - kx0);
+  if (tid == 0) mbar_init(bar, 1);
+  __syncthreads();
+  if (tid == 0) {
+    mbar_expect_tx(bar, (uint32_t)(m * N * B * sizeof(V)));
+    for (int s = 0; s < m; ++s) tma_load_3d(buf + s * N * B, &tm, bar, 2 * kx0, y, s * g.N2);
+  }
+  for (int q = tid; q < N; q += NTHR) tw[q] = twg[q];
+  if (!mbar_wait(bar, 0, kMbarPolls)) {
+    if (tid == 0) atomicExch(err, 2);
+    return;
+  }
+  __syncthreads();
+  for (int s = 0; s < m; ++s) fft2<N, B, NTHR, false, true, LayCol<N, B>>(buf + s * N * B, tw);
+  const int ky = kfreq(y, g.N1);
+  const double k1 = ky * g.dk1;
+  const long long zstride = (long long)g.N1 * g.Nhp;
+  const long long col = (long long)y * g.Nhp + kx0;
+#pragma unroll 1
+  for (int e = tid; e < N * B; e += NTHR) {
+    const int z = e / B, b = e % B;
+    if (b >= bw) continue;
+    const int kx = kx0 + b;
+    const int kz = kfreq(z, N);
+    const double k0 = kx * g.dk0, k2 = kz * g.dk2;
+    const double kk = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(k0, k0), __dmul_rn(k1, k1)), __dmul_rn(k2, k2)));
+    const double ix = kk / zp.dkr - 0.5;
+    int i = (int)(ix + 0.5);
+    i = min(max(i, 0), zp.nrad - 1);
+    const T fr = T(ix - i);
+    V c[MS];
+#pragma unroll
+    for (int j = 0; j < MS; ++j)
+      if (j < m) c[j] = buf[j * N * B + e];
+    V Lk;
+    Lk.x = T(0); Lk.y = T(0);
+    if (MODE == MODE_F && zp.L != nullptr) {
+      Lk = zp.L[z * zstride + col + b];
+#pragma unroll
+      for (int j = 0; j < MS; ++j)
+        if (j < m) { c[j].x -= zp.a[j] * Lk.x; c[j].y -= zp.a[j] * Lk.y; }
+    }
+#pragma unroll
+    for (int ii = 0; ii < MS; ++ii) {
+      if (ii < m) {
+        V t;
+        t.x = T(0); t.y = T(0);
+#pragma unroll
+        for (int j = 0; j < MS; ++j) {
+          if (j < m) {
+            const int pidx = ii >= j ? ii * (ii + 1) / 2 + j : j * (j + 1) / 2 + ii;
+            const P2 tv = zp.chi[(long long)pidx * zp.nrad + i];
+            const T x = tv.x + tv.y * fr;
+            t.x += x * c[j].x;
+            t.y += x * c[j].y;
+          }
+        }
+        if (MODE == MODE_F && zp.L != nullptr) {
+          T bb = zp.bconst[ii];
+          if (zp.stab != nullptr) {
+            const P2 sv = zp.stab[(long long)ii * zp.nrad + i];
+            bb += sv.x + sv.y * fr;
+          }
+          t.x -= bb * Lk.x;
+          t.y -= bb * Lk.y;
+        }
+        buf[ii * N * B + e] = t;
+      }
+    }
+  }
+  __syncthreads();
+  for (int s = 0; s < m; ++s) fft2<N, B, NTHR, true, true, LayCol<N, B>>(buf + s * N * B, tw);
+  fence_proxy_async();
+  __syncthreads();
+  if (tid == 0) {
+    for (int s = 0; s < m; ++s) tma_store_3d(&tm, buf + s * N * B, 2 * kx0, y, s * g.N2);
+    tma_commit();
+    tma_wait_read0();
+  }
+}
+
+}  // namespace rism

@@ -5,6 +5,8 @@
 // Reference: hnc3d_solute_solve (hnc3d.c:1762-2350) driving iterate_t1 /
 // jacobian_t1 (hnc3d.c:1183-1362) through bgy3d_snes_newton
 // (bgy3d-snes.c:160-346, SNESNEWTONLS + KSPGMRES(30), KSP rtol = 100 * 1e-5).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -17,6 +19,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "kernels_static.cuh"
 #include "rism3d.h"
 
 using namespace rism;
@@ -164,13 +167,19 @@ struct rism3d_ctx {
   PassTimer timer;
   int f_evals = 0, jv_evals = 0, f32_evals = 0, jv32_evals = 0;
 
+  // shape-specialised passes: available per precision ([0] FP64, [1] FP32),
+  // with TMA descriptors of W for the y and z tiles
+  bool stat[2] = {false, false};
+  CUtensorMap tmy[2], tmz[2];
+  int *d_err = nullptr;  // set by a kernel whose bounded wait timed out
+
   ~rism3d_ctx() {
     auto fr = [](void *p) { if (p) cudaFree(p); };
     for (int i = 0; i < 3; ++i) { fr(tw64[i]); fr(tw32[i]); }
     fr(post64); fr(post32); fr(v64); fr(v32); fr(L64); fr(L32);
     fr(chi64); fr(s64); fr(chi32); fr(s32); fr(W); fr(d_solute); fr(d_charge);
     fr(npart); fr(dpart); fr(F64); fr(X64t); fr(F64t); fr(X32); fr(F32); fr(X32t); fr(F32t);
-    fr(d64); fr(d32); fr(dx64); fr(dx32);
+    fr(d64); fr(d32); fr(dx64); fr(dx32); fr(d_err);
     for (auto p : basis64) fr(p);
     for (auto p : basis32) fr(p);
     if (timer.on) { cudaEventDestroy(timer.a); cudaEventDestroy(timer.b); }
@@ -253,11 +262,76 @@ template <typename T> size_t zsmem(rism3d_ctx *c) {
   return sizeof(typename Cx<T>::type) * (size_t)(c->g.N2 + c->g.N2 * c->m * c->tl<T>().BZ);
 }
 
+// ---- shape-specialised passes
+constexpr int kStaticRX = 16;
+// y/z tile width: 128-byte rows (16 float2 or 8 double2)
+template <typename T> constexpr int static_B() { return sizeof(T) == 4 ? 16 : 8; }
+template <typename T, int M> constexpr size_t xs_smem() {
+  return sizeof(typename Cx<T>::type) * (size_t)(M + kStaticRX * (M + M / Split<M>::R2));
+}
+template <typename T, int N> constexpr size_t ys_smem() {
+  return sizeof(typename Cx<T>::type) * (size_t)(N * static_B<T>() + N) + 16;
+}
+template <typename T, int N> size_t zs_smem(int m) {
+  return sizeof(typename Cx<T>::type) * (size_t)(m * N * static_B<T>() + N) + 16;
+}
+bool static_len_x(int M) { return M == 48 || M == 64 || M == 128; }
+bool static_len_yz(int N) { return N == 96 || N == 128 || N == 256; }
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    CK(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !p) {
+      g_last_error = "cuTensorMapEncodeTiled unavailable";
+      throw CudaFail{RISM3D_ERR_CUDA};
+    }
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// W viewed as a 3D tensor of scalars {2 Nhp, N1, m N2}; box {2B, by, bz}.
+void make_tmap(rism3d_ctx *c, CUtensorMap *tm, bool fp64, int B, int by, int bz) {
+  const Geo &G = c->g;
+  const size_t es = fp64 ? 8 : 4;
+  cuuint64_t dims[3] = {(cuuint64_t)(2 * G.Nhp), (cuuint64_t)G.N1, (cuuint64_t)G.N2 * G.m};
+  cuuint64_t strides[2] = {(cuuint64_t)(2 * G.Nhp) * es, (cuuint64_t)(2 * G.Nhp) * G.N1 * es};
+  cuuint32_t box[3] = {(cuuint32_t)(2 * B), (cuuint32_t)by, (cuuint32_t)bz};
+  cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = encode_fn()(tm, fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                                 c->W, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    g_last_error = "cuTensorMapEncodeTiled failed: " + std::to_string((int)r);
+    throw CudaFail{RISM3D_ERR_CUDA};
+  }
+}
+
 template <typename T, bool INV> void launch_y(rism3d_ctx *c) {
   TimeScope ts(c, TK_Y, sizeof(T) == 8 ? 0 : 1);
+  auto *W = c->work<T>();
+  if (c->stat[sizeof(T) == 8 ? 0 : 1]) {
+    constexpr int B = static_B<T>();
+    dim3 grid((c->g.Nh + B - 1) / B, c->g.N2, c->m);
+    const CUtensorMap &tm = c->tmy[sizeof(T) == 8 ? 0 : 1];
+    const auto *tw = static_cast<const typename Cx<T>::type *>(c->plan<T>(1).tw);
+    switch (c->g.N1) {
+#define Y_CASE(N)                                                                                   \
+  case N:                                                                                           \
+    k_y_s<T, INV, N, B><<<grid, Split<N>::R1 * B, ys_smem<T, N>(), c->stream>>>(c->g, tm, tw, c->d_err); \
+    break;
+      Y_CASE(96) Y_CASE(128) Y_CASE(256)
+#undef Y_CASE
+    }
+    CKL();
+    return;
+  }
   dim3 grid((c->g.Nh + c->tl<T>().BY - 1) / c->tl<T>().BY, c->g.N2, c->m);
   const size_t sm = ysmem<T>(c);
-  auto *W = c->work<T>();
   if (c->tl<T>().BY == 16) k_y<T, INV, 16><<<grid, 256, sm, c->stream>>>(c->g, c->plan<T>(1), W);
   else if (c->tl<T>().BY == 8) k_y<T, INV, 8><<<grid, 256, sm, c->stream>>>(c->g, c->plan<T>(1), W);
   else k_y<T, INV, 4><<<grid, 256, sm, c->stream>>>(c->g, c->plan<T>(1), W);
@@ -266,10 +340,27 @@ template <typename T, bool INV> void launch_y(rism3d_ctx *c) {
 
 template <typename T, int MODE> void launch_z(rism3d_ctx *c) {
   TimeScope ts(c, TK_Z, sizeof(T) == 8 ? 0 : 1);
-  dim3 grid((c->g.Nh + c->tl<T>().BZ - 1) / c->tl<T>().BZ, c->g.N1);
-  const size_t sm = zsmem<T>(c);
   auto *W = c->work<T>();
   const ZParams<T> zp = zparams<T>(c, MODE == MODE_F);
+  if (c->stat[sizeof(T) == 8 ? 0 : 1]) {
+    constexpr int B = static_B<T>();
+    dim3 grid((c->g.Nh + B - 1) / B, c->g.N1);
+    const CUtensorMap &tm = c->tmz[sizeof(T) == 8 ? 0 : 1];
+    const auto *tw = static_cast<const typename Cx<T>::type *>(c->plan<T>(2).tw);
+    switch (c->g.N2) {
+#define Z_CASE(N)                                                                                        \
+  case N:                                                                                                \
+    k_z_s<T, MODE, N, B, 3><<<grid, Split<N>::R1 * B, zs_smem<T, N>(c->m), c->stream>>>(c->g, tm, tw, zp, \
+                                                                                          c->d_err);     \
+    break;
+      Z_CASE(96) Z_CASE(128) Z_CASE(256)
+#undef Z_CASE
+    }
+    CKL();
+    return;
+  }
+  dim3 grid((c->g.Nh + c->tl<T>().BZ - 1) / c->tl<T>().BZ, c->g.N1);
+  const size_t sm = zsmem<T>(c);
   if (c->tl<T>().BZ == 16) k_z<T, MODE, 16><<<grid, 256, sm, c->stream>>>(c->g, c->plan<T>(2), W, zp);
   else if (c->tl<T>().BZ == 8) k_z<T, MODE, 8><<<grid, 256, sm, c->stream>>>(c->g, c->plan<T>(2), W, zp);
   else k_z<T, MODE, 4><<<grid, 256, sm, c->stream>>>(c->g, c->plan<T>(2), W, zp);
@@ -280,7 +371,13 @@ void reduce_norms(rism3d_ctx *c, int nblk, double *resid) {
   c->h_npart.resize(nblk);
   CK(cudaMemcpyAsync(c->h_npart.data(), c->npart, sizeof(NormPartial) * nblk, cudaMemcpyDeviceToHost,
                      c->stream));
+  int err = 0;
+  CK(cudaMemcpyAsync(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (err) {
+    g_last_error = "a bounded TMA/mbarrier wait timed out in pass " + std::to_string(err);
+    throw CudaFail{RISM3D_ERR_CUDA};
+  }
   double amax = 0.0, s2 = 0.0;
   for (int i = 0; i < nblk; ++i) {
     const double a = c->h_npart[i].amax;
@@ -291,52 +388,72 @@ void reduce_norms(rism3d_ctx *c, int nblk, double *resid) {
   resid[1] = std::sqrt(s2);
 }
 
-// F(x) -> out (iterate_t1).  resid: ||out||_inf, ||out||_2 (host), or null.
-template <typename T> void eval_F(rism3d_ctx *c, const T *x, T *out, double *resid) {
+// The five passes of one residual (MODE_F: A = t, Bv = v, p = beta) or
+// Jacobian product (MODE_J: A = dt, Bv = d = c'(t), p = scale of dt);
+// out = (FFT^-1 ...) / N - sub * A.  Returns the number of norm partials.
+template <typename T, int MODE>
+int pipeline(rism3d_ctx *c, const T *A, const T *Bv, T p, T sub, T *out) {
   const int rows = c->g.N1 * c->g.N2;
-  dim3 gx((rows + c->tl<T>().RX - 1) / c->tl<T>().RX, c->m);
   auto *W = c->work<T>();
+  const bool st = c->stat[sizeof(T) == 8 ? 0 : 1];
+  const int RX = st ? kStaticRX : c->tl<T>().RX;
+  dim3 gx((rows + RX - 1) / RX, c->m);
+  const auto *twx = static_cast<const typename Cx<T>::type *>(c->plan<T>(0).tw);
   {
     TimeScope ts(c, TK_XFWD, sizeof(T) == 8 ? 0 : 1);
-    k_xfwd<T, MODE_F><<<gx, 256, xsmem<T>(c), c->stream>>>(c->g, c->plan<T>(0), c->tl<T>().RX, x, vfield<T>(c),
-                                                          (T)c->pd.beta, c->pd.closure, W, postw<T>(c));
+    if (st) {
+      switch (c->g.M) {
+#define XF_CASE(M)                                                                                     \
+  case M:                                                                                              \
+    k_xfwd_s<T, MODE, M, kStaticRX><<<gx, 256, xs_smem<T, M>(), c->stream>>>(c->g, A, Bv, p, c->pd.closure, \
+                                                                             W, postw<T>(c), twx);      \
+    break;
+        XF_CASE(48) XF_CASE(64) XF_CASE(128)
+#undef XF_CASE
+      }
+    } else {
+      k_xfwd<T, MODE><<<gx, 256, xsmem<T>(c), c->stream>>>(c->g, c->plan<T>(0), RX, A, Bv, p, c->pd.closure, W,
+                                                          postw<T>(c));
+    }
     CKL();
   }
   launch_y<T, false>(c);
-  launch_z<T, MODE_F>(c);
+  launch_z<T, MODE>(c);
   launch_y<T, true>(c);
   {
     TimeScope ts(c, TK_XINV, sizeof(T) == 8 ? 0 : 1);
-    k_xinv<T><<<gx, 256, xsmem<T>(c), c->stream>>>(c->g, c->plan<T>(0), c->tl<T>().RX, W, x, out,
-                                                   (T)(1.0 / (double)c->g.Nr), (T)1, postw<T>(c), c->npart);
+    const T scale = (T)(1.0 / (double)c->g.Nr);
+    if (st) {
+      switch (c->g.M) {
+#define XI_CASE(M)                                                                                            \
+  case M:                                                                                                     \
+    k_xinv_s<T, M, kStaticRX><<<gx, 256, xs_smem<T, M>(), c->stream>>>(c->g, W, A, out, scale, sub, postw<T>(c), \
+                                                                       twx, c->npart);                        \
+    break;
+        XI_CASE(48) XI_CASE(64) XI_CASE(128)
+#undef XI_CASE
+      }
+    } else {
+      k_xinv<T><<<gx, 256, xsmem<T>(c), c->stream>>>(c->g, c->plan<T>(0), RX, W, A, out, scale, sub, postw<T>(c),
+                                                     c->npart);
+    }
     CKL();
   }
+  return gx.x * gx.y;
+}
+
+// F(x) -> out (iterate_t1).  resid: ||out||_inf, ||out||_2 (host), or null.
+template <typename T> void eval_F(rism3d_ctx *c, const T *x, T *out, double *resid) {
+  const int nb = pipeline<T, MODE_F>(c, x, vfield<T>(c), (T)c->pd.beta, (T)1, out);
   if (sizeof(T) == 8) c->f_evals++; else c->f32_evals++;
-  if (resid) reduce_norms(c, gx.x * gx.y, resid);
+  if (resid) reduce_norms(c, nb, resid);
 }
 
 // out = J(x0) (s * vin) with d = c'(x0) precomputed (jacobian_t1).
 template <typename T> void eval_J(rism3d_ctx *c, const T *d, const T *vin, double s, T *out, double *resid) {
-  const int rows = c->g.N1 * c->g.N2;
-  dim3 gx((rows + c->tl<T>().RX - 1) / c->tl<T>().RX, c->m);
-  auto *W = c->work<T>();
-  {
-    TimeScope ts(c, TK_XFWD, sizeof(T) == 8 ? 0 : 1);
-    k_xfwd<T, MODE_J><<<gx, 256, xsmem<T>(c), c->stream>>>(c->g, c->plan<T>(0), c->tl<T>().RX, vin, d, (T)s,
-                                                          c->pd.closure, W, postw<T>(c));
-    CKL();
-  }
-  launch_y<T, false>(c);
-  launch_z<T, MODE_J>(c);
-  launch_y<T, true>(c);
-  {
-    TimeScope ts(c, TK_XINV, sizeof(T) == 8 ? 0 : 1);
-    k_xinv<T><<<gx, 256, xsmem<T>(c), c->stream>>>(c->g, c->plan<T>(0), c->tl<T>().RX, W, vin, out,
-                                                   (T)(1.0 / (double)c->g.Nr), (T)s, postw<T>(c), c->npart);
-    CKL();
-  }
+  const int nb = pipeline<T, MODE_J>(c, vin, d, (T)s, (T)s, out);
   if (sizeof(T) == 8) c->jv_evals++; else c->jv32_evals++;
-  if (resid) reduce_norms(c, gx.x * gx.y, resid);
+  if (resid) reduce_norms(c, nb, resid);
 }
 
 int vec_grid(long long n) {
@@ -870,8 +987,21 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
     CK(cudaMalloc(&c->W, sizeof(double2) * (size_t)(m * G.Nc)));
     c->dpart = dalloc<double>((size_t)c->red_blocks * kDotChunk + 64);
     const int rows = G.N1 * G.N2;
-    const int rxmin = std::min(c->tiles[0].RX, c->tiles[1].RX);
+    const int rxmin = std::min(std::min(c->tiles[0].RX, c->tiles[1].RX), kStaticRX);
     c->npart = dalloc<NormPartial>((size_t)((rows + rxmin - 1) / rxmin) * m);
+    c->d_err = dalloc<int>(1);
+    CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    // shape-specialised passes (TMA tiles) for the lengths they are built for;
+    // RISM3D_GENERIC_PASSES=1 selects the runtime-length passes everywhere
+    const char *gen = std::getenv("RISM3D_GENERIC_PASSES");
+    if (static_len_x(G.M) && static_len_yz(G.N1) && static_len_yz(G.N2) && m <= 3 && !(gen && gen[0] == '1')) {
+      for (int pr = 0; pr < 2; ++pr) {
+        const int B = pr == 0 ? static_B<double>() : static_B<float>();
+        make_tmap(c, &c->tmy[pr], pr == 0, B, G.N1, 1);
+        make_tmap(c, &c->tmz[pr], pr == 0, B, 1, G.N2);
+        c->stat[pr] = true;
+      }
+    }
     // shared-memory opt-in: each kernel may use the device's per-block
     // opt-in limit minus its own static shared memory
     int dev = 0, optin = 0;
@@ -910,6 +1040,35 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
     OPTIN_YZ(double)
     OPTIN_YZ(float)
 #undef OPTIN_YZ
+    if (c->stat[0]) {
+      need = std::max({xs_smem<double, 128>(), ys_smem<double, 256>(), zs_smem<double, 256>(m),
+                       xs_smem<float, 128>(), ys_smem<float, 256>(), zs_smem<float, 256>(m)});
+#define OPTIN_S(T)                                                                          \
+  allow((const void *)k_xfwd_s<T, MODE_F, 48, kStaticRX>);                                  \
+  allow((const void *)k_xfwd_s<T, MODE_J, 48, kStaticRX>);                                  \
+  allow((const void *)k_xfwd_s<T, MODE_F, 64, kStaticRX>);                                  \
+  allow((const void *)k_xfwd_s<T, MODE_J, 64, kStaticRX>);                                  \
+  allow((const void *)k_xfwd_s<T, MODE_F, 128, kStaticRX>);                                 \
+  allow((const void *)k_xfwd_s<T, MODE_J, 128, kStaticRX>);                                 \
+  allow((const void *)k_xinv_s<T, 48, kStaticRX>);                                          \
+  allow((const void *)k_xinv_s<T, 64, kStaticRX>);                                          \
+  allow((const void *)k_xinv_s<T, 128, kStaticRX>);                                         \
+  allow((const void *)k_y_s<T, false, 96, static_B<T>()>);                                  \
+  allow((const void *)k_y_s<T, true, 96, static_B<T>()>);                                   \
+  allow((const void *)k_y_s<T, false, 128, static_B<T>()>);                                 \
+  allow((const void *)k_y_s<T, true, 128, static_B<T>()>);                                  \
+  allow((const void *)k_y_s<T, false, 256, static_B<T>()>);                                 \
+  allow((const void *)k_y_s<T, true, 256, static_B<T>()>);                                  \
+  allow((const void *)k_z_s<T, MODE_F, 96, static_B<T>(), 3>);                              \
+  allow((const void *)k_z_s<T, MODE_J, 96, static_B<T>(), 3>);                              \
+  allow((const void *)k_z_s<T, MODE_F, 128, static_B<T>(), 3>);                             \
+  allow((const void *)k_z_s<T, MODE_J, 128, static_B<T>(), 3>);                             \
+  allow((const void *)k_z_s<T, MODE_F, 256, static_B<T>(), 3>);                             \
+  allow((const void *)k_z_s<T, MODE_J, 256, static_B<T>(), 3>);
+      OPTIN_S(double)
+      OPTIN_S(float)
+#undef OPTIN_S
+    }
   } catch (...) {
     delete c;
     throw;

@@ -124,6 +124,47 @@ def test_solve_matches_oracle(case, precision):
     ctx2.close()
 
 
+@pytest.fixture(scope="module")
+def static_cases(fixture_loader):
+    """Grids served by the shape-specialised (TMA) passes: the README water
+    case at 96^3 and a 5-site synthetic solute at 128^3."""
+    from bgy3d_b200 import find_molecule, rism_solvent, synthetic_solute
+    meta, arr = fixture_loader("water_readme_n96")
+    out = [(meta["solute"], meta["solvent"], settings_of(meta), arr["chi"])]
+    water = find_molecule("water, PR-SPC/E")
+    s = {"L": 16.0, "N": 128, "rho": 0.0333295, "beta": 1.6889, "closure": "KH", "rmax": 40.0,
+         "nrad": 1024, "dielectric": 78.4}
+    chi = rism_solvent(water, dict(s, **{"norm-tol": 1e-12}))["susceptibility"]
+    out.append((synthetic_solute(5, radius=3.0, seed=20261204), water, s, chi))
+    return out
+
+
+@pytest.mark.parametrize("which", [0, 1])
+def test_static_passes_match_oracle(static_cases, which, monkeypatch):
+    solute, solvent, s, chi = static_cases[which]
+    ctx = RismContext(solute, solvent, s, chi)
+    monkeypatch.setenv("RISM3D_GENERIC_PASSES", "1")
+    gen = RismContext(solute, solvent, s, chi)
+    monkeypatch.delenv("RISM3D_GENERIC_PASSES")
+    N = s["N"]
+    clo = cl.NAMES[s["closure"]] if isinstance(s["closure"], str) else int(s["closure"])
+    P = hnc3d.Problem((N,) * 3, (2 * s["L"],) * 3, s["beta"], s["rho"], clo, solvent, solute, chi, s["rmax"])
+    rng = np.random.default_rng(5)
+    T = 0.3 * rng.standard_normal(ctx.shape)
+    dT = rng.standard_normal(ctx.shape)
+    F_ref = P.iterate_t1(T)
+    J_ref = P.jacobian_t1(T, dT)
+    for dt, tol in ((torch.float64, 1e-11), (torch.float32, 2e-5)):
+        F = ctx.iterate_t1(to_dev(T, dt))[0].double().cpu().numpy()
+        J = ctx.jacobian_t1(to_dev(T, dt), to_dev(dT, dt)).double().cpu().numpy()
+        assert np.max(np.abs(F - F_ref)) < tol * np.max(np.abs(F_ref)), dt
+        assert np.max(np.abs(J - J_ref)) < tol * np.max(np.abs(J_ref)), dt
+        Fg = gen.iterate_t1(to_dev(T, dt))[0].double().cpu().numpy()
+        assert np.max(np.abs(F - Fg)) < tol * np.max(np.abs(F_ref)), dt
+    ctx.close()
+    gen.close()
+
+
 def test_host_entry_point_and_restart(fixture_loader):
     meta, arr = fixture_loader("water_hnc_n24")
     s = settings_of(meta, **{"norm-tol": 1e-12})
