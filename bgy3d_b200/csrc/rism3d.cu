@@ -696,7 +696,8 @@ NewtonOut newton(rism3d_ctx *c, TS *x, double tol, int max_iter, double krylov_r
     o.iters = it + 1;
     closure_slope<TS, TJ>(c, x, d);
     axpby<TS, TJ>(c, -1.0, F, 0.0, rhs);
-    gmres<TJ>(c, d, rhs, dx, krylov_rtol, 1000, restart);
+    const int kits = gmres<TJ>(c, d, rhs, dx, krylov_rtol, 1000, restart);
+    if (c->pd.verbosity > 0) std::fprintf(stderr, "   gmres: %d J.v\n", kits);
     const double f0 = r[1] * r[1];
     double lam = 1.0, f1 = 0.0, rt[2] = {0, 0};
     bool decreased = false;
