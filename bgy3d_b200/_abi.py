@@ -58,7 +58,7 @@ EXPORTS = [
     "rism3d_ctx_destroy", "rism3d_ctx_size", "rism3d_iterate_t1",
     "rism3d_jacobian_t1", "rism3d_iterate_t1_f32", "rism3d_jacobian_t1_f32",
     "rism3d_solve", "rism3d_observables", "rism3d_get_field", "rism3d_last_error",
-    "rism3d_profile", "rism1d_solvent_chi",
+    "rism3d_profile", "rism1d_solvent_chi", "rism3d_jacobian_apply_noalloc",
 ]
 
 _lib = None
@@ -101,6 +101,8 @@ def lib():
     L.rism3d_profile.restype = I
     L.rism1d_solvent_chi.argtypes = [P(Problem), D, I, P(Site), P(D), P(D), P(D)]
     L.rism1d_solvent_chi.restype = I
+    L.rism3d_jacobian_apply_noalloc.argtypes = [P(Problem), I, P(D), V, V, V]
+    L.rism3d_jacobian_apply_noalloc.restype = I
     _lib = L
     return L
 

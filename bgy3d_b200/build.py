@@ -13,8 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librism3d.so")
-SOURCES = ["rism3d.cu", "rism1d.cpp"]
-HEADERS = ["fft_core.cuh", "kernels.cuh"]
+SOURCES = ["rism3d.cu", "rism1d.cpp", "noalloc.cu"]
+HEADERS = ["fft_core.cuh", "kernels.cuh", "fft_static.cuh", "kernels_static.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 

@@ -427,7 +427,7 @@ __device__ __forceinline__ double cl0(double r) {     // bgy3d-solutes.c:147-159
 
 // v[i][p] = sum_u eps_iu ljcap0(r/sigma_iu) + q_i q_u/eps0 G cscap0(G r)
 // (field0, bgy3d-solutes.c:343-377); grid point r = i h - L/2.
-__global__ void k_field0(Geo g, double h0, double h1, double h2, double L0, double L1, double L2,
+static __global__ void k_field0(Geo g, double h0, double h1, double h2, double L0, double L1, double L2,
                          const SiteP *__restrict__ solvent, int n, const SiteP *__restrict__ solute,
                          double *__restrict__ v) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -453,7 +453,7 @@ __global__ void k_field0(Geo g, double h0, double h1, double h2, double L0, doub
 }
 
 // uc(r) = (1/eps0) sum_u q_u G cl0(G r) (coulomb_long, bgy3d-solutes.c:795-815).
-__global__ void k_coulomb_long(Geo g, double h0, double h1, double h2, double L0, double L1, double L2,
+static __global__ void k_coulomb_long(Geo g, double h0, double h1, double h2, double L0, double L1, double L2,
                                int n, const SiteP *__restrict__ solute, double *__restrict__ uc) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= g.Nr) return;
@@ -474,7 +474,7 @@ __global__ void k_coulomb_long(Geo g, double h0, double h1, double h2, double L0
 // F(k) = sum_u q_u exp(-i k.x_u) (-1)^(kx+ky+kz).  renorm: L = F / h^3;
 // no-renorm: L = (4 pi/eps0) exp(-k^2/4G^2)/k^2 F / h^3 (coulomb_long_fft,
 // bgy3d-solutes.c:766-792; zero at k = 0).  Written in FP64 and FP32.
-__global__ void k_longrange(Geo g, int n, const SiteP *__restrict__ solute, int renorm, double inv_h3,
+static __global__ void k_longrange(Geo g, int n, const SiteP *__restrict__ solute, int renorm, double inv_h3,
                             double2 *__restrict__ L64, float2 *__restrict__ L32) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long tot = (long long)g.Nh * g.N1 * g.N2;
@@ -516,7 +516,7 @@ __global__ void k_closure_slope(long long n, long long Nr, const double *__restr
 // densities by the native, HNC, KH and GF functionals and of c; g = h + 1.
 struct ObsPartial { double mu, hnc, kh, gf, csum; };
 
-__global__ void k_observables(Geo g, const double *__restrict__ t, const double *__restrict__ v,
+static __global__ void k_observables(Geo g, const double *__restrict__ t, const double *__restrict__ v,
                               const double *__restrict__ uc, double beta, int closure,
                               const double *__restrict__ charge, double *__restrict__ gout,
                               ObsPartial *__restrict__ part) {

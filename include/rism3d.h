@@ -182,6 +182,23 @@ const char *rism3d_last_error(void);
    1 for FP32.  Launches are counted even when timing is off. */
 int rism3d_profile(rism3d_ctx *ctx, int on, double *ms, long long *launches);
 
+/* Jacobian product J dT = (chi - 1) * (d . dT) - dT for a caller-supplied
+   closure slope d = dc/dt at the current t ([m][N2][N1][N0], device, FP64),
+   computed by the same passes as rism3d_jacobian_t1 -- but allocating no
+   device memory.  It has no counterpart in the reference: it exists for
+   callers that cannot call cudaMalloc (solver loops where an allocation
+   would synchronise the device or is forbidden by the host framework, or
+   code that owns every device buffer itself).  Its scratch lives in a
+   32 MiB file-scope device array held by every device that loads the
+   library until exit; grids whose scratch exceeds it return RISM3D_ERR_ARG
+   (m = 3 fits up to 96^3).  chi is the host [m][m][nrad] table as for
+   rism3d_ctx_create; dT, JdT are device pointers; default stream, returns
+   after the result is complete.  The first call on a device looks up the
+   array's device address (make it before any stream capture).  All calls
+   share the array: calls that overlap on the GPU race. */
+int rism3d_jacobian_apply_noalloc(const rism3d_problem *pd, int m, const double *chi,
+                                  const double *d, const double *dT, double *JdT);
+
 /* ---- solvent susceptibility (setup, CPU) ------------------------------ */
 
 /* 1D RISM / DRISM of the pure solvent: replaces rism_solvent()
