@@ -42,19 +42,31 @@ __global__ void __launch_bounds__(256) k_xfwd_s(Geo g, const T *__restrict__ A, 
   for (int q = tid; q < M; q += 256) tw[q] = twg[q];
   const long long sbase = (long long)site * g.Nr;
   constexpr int PER_ROW = M / VW;
-#pragma unroll 4
-  for (int e = tid; e < RX * PER_ROW; e += 256) {
+  constexpr int CNT = (RX * PER_ROW + 255) / 256;
+  // all loads of the thread in flight before any use
+  VEC ra[CNT], rb[CNT];
+#pragma unroll
+  for (int it = 0; it < CNT; ++it) {
+    const int e = tid + it * 256;
+    const int row = e / PER_ROW, jj = (e % PER_ROW) * VW;
+    if (e < RX * PER_ROW && row0 + row < rows_total) {
+      const long long off = sbase + (long long)(row0 + row) * g.N0 + 2 * jj;
+      ra[it] = *reinterpret_cast<const VEC *>(A + off);
+      rb[it] = *reinterpret_cast<const VEC *>(Bv + off);
+    }
+  }
+#pragma unroll
+  for (int it = 0; it < CNT; ++it) {
+    const int e = tid + it * 256;
+    if (e >= RX * PER_ROW) break;
     const int row = e / PER_ROW, jj = (e % PER_ROW) * VW;
     const int grow = row0 + row;
     V z[VW];
 #pragma unroll
     for (int v = 0; v < VW; ++v) z[v].x = z[v].y = T(0);
     if (grow < rows_total) {
-      const long long off = sbase + (long long)grow * g.N0 + 2 * jj;
-      const VEC a = *reinterpret_cast<const VEC *>(A + off);
-      const VEC b = *reinterpret_cast<const VEC *>(Bv + off);
-      const T *ar = reinterpret_cast<const T *>(&a);
-      const T *br = reinterpret_cast<const T *>(&b);
+      const T *ar = reinterpret_cast<const T *>(&ra[it]);
+      const T *br = reinterpret_cast<const T *>(&rb[it]);
 #pragma unroll
       for (int v = 0; v < VW; ++v) {
         if (MODE == MODE_F) {
@@ -112,6 +124,19 @@ __global__ void __launch_bounds__(256) k_xinv_s(Geo g, const typename Cx<T>::typ
   for (int q = tid; q < M; q += 256) tw[q] = twg[q];
   constexpr int H = M / 2 + 1;
   const long long wbase = (long long)site * g.Nc;
+  const long long sbase = (long long)site * g.Nr;
+  constexpr int PER_ROW = M / VW;
+  constexpr int CNT = (RX * PER_ROW + 255) / 256;
+  // the subtracted input is fetched first; its latency hides behind the
+  // transform
+  VEC rin[CNT];
+#pragma unroll
+  for (int it = 0; it < CNT; ++it) {
+    const int e = tid + it * 256;
+    const int row = e / PER_ROW, jj = (e % PER_ROW) * VW;
+    if (e < RX * PER_ROW && row0 + row < rows_total)
+      rin[it] = *reinterpret_cast<const VEC *>(In + sbase + (long long)(row0 + row) * g.N0 + 2 * jj);
+  }
 #pragma unroll 2
   for (int e = tid; e < RX * H; e += 256) {
     const int row = e / H, k = e % H;
@@ -136,16 +161,15 @@ __global__ void __launch_bounds__(256) k_xinv_s(Geo g, const typename Cx<T>::typ
   __syncthreads();
   fft2<M, RX, 256, true, false, Lay>(buf, tw);
   double amax = 0.0, sum2 = 0.0;
-  const long long sbase = (long long)site * g.Nr;
-  constexpr int PER_ROW = M / VW;
-#pragma unroll 4
-  for (int e = tid; e < RX * PER_ROW; e += 256) {
+#pragma unroll
+  for (int it = 0; it < CNT; ++it) {
+    const int e = tid + it * 256;
+    if (e >= RX * PER_ROW) break;
     const int row = e / PER_ROW, jj = (e % PER_ROW) * VW;
     const int grow = row0 + row;
     if (grow >= rows_total) continue;
     const long long off = sbase + (long long)grow * g.N0 + 2 * jj;
-    const VEC in = *reinterpret_cast<const VEC *>(In + off);
-    const T *ir = reinterpret_cast<const T *>(&in);
+    const T *ir = reinterpret_cast<const T *>(&rin[it]);
     VEC o;
     T *orr = reinterpret_cast<T *>(&o);
 #pragma unroll
@@ -236,10 +260,15 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_z_s(Geo g, const __grid_co
   const double k1 = ky * g.dk1;
   const long long zstride = (long long)g.N1 * g.Nhp;
   const long long col = (long long)y * g.Nhp + kx0;
-#pragma unroll 1
+  // contraction: all table entries of an element are fetched before use and
+  // two elements are in flight per thread (the tables live in L1/L2)
+  constexpr int NP = MS * (MS + 1) / 2;
+  const int np = m * (m + 1) / 2;
+  const bool full = MODE == MODE_F && zp.L != nullptr;
+#pragma unroll 2
   for (int e = tid; e < N * B; e += NTHR) {
     const int z = e / B, b = e % B;
-    if (b >= bw) continue;
+    const bool valid = b < bw;
     const int kx = kx0 + b;
     const int kz = kfreq(z, N);
     const double k0 = kx * g.dk0, k2 = kz * g.dk2;
@@ -248,18 +277,34 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_z_s(Geo g, const __grid_co
     int i = (int)(ix + 0.5);
     i = min(max(i, 0), zp.nrad - 1);
     const T fr = T(ix - i);
+    P2 tv[NP];
+#pragma unroll
+    for (int q = 0; q < NP; ++q)
+      if (q < np) tv[q] = __ldg(&zp.chi[(long long)q * zp.nrad + i]);
+    P2 sv[MS];
+    V Lk;
+    Lk.x = T(0); Lk.y = T(0);
+    if (full) {
+      if (zp.stab != nullptr) {
+#pragma unroll
+        for (int ii = 0; ii < MS; ++ii)
+          if (ii < m) sv[ii] = __ldg(&zp.stab[(long long)ii * zp.nrad + i]);
+      }
+      if (valid) Lk = __ldg(&zp.L[z * zstride + col + b]);
+    }
     V c[MS];
 #pragma unroll
     for (int j = 0; j < MS; ++j)
       if (j < m) c[j] = buf[j * N * B + e];
-    V Lk;
-    Lk.x = T(0); Lk.y = T(0);
-    if (MODE == MODE_F && zp.L != nullptr) {
-      Lk = zp.L[z * zstride + col + b];
+    if (full) {
 #pragma unroll
       for (int j = 0; j < MS; ++j)
         if (j < m) { c[j].x -= zp.a[j] * Lk.x; c[j].y -= zp.a[j] * Lk.y; }
     }
+    T xv[NP];
+#pragma unroll
+    for (int q = 0; q < NP; ++q)
+      if (q < np) xv[q] = tv[q].x + tv[q].y * fr;
 #pragma unroll
     for (int ii = 0; ii < MS; ++ii) {
       if (ii < m) {
@@ -268,23 +313,18 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_z_s(Geo g, const __grid_co
 #pragma unroll
         for (int j = 0; j < MS; ++j) {
           if (j < m) {
-            const int pidx = ii >= j ? ii * (ii + 1) / 2 + j : j * (j + 1) / 2 + ii;
-            const P2 tv = zp.chi[(long long)pidx * zp.nrad + i];
-            const T x = tv.x + tv.y * fr;
+            const T x = xv[ii >= j ? ii * (ii + 1) / 2 + j : j * (j + 1) / 2 + ii];
             t.x += x * c[j].x;
             t.y += x * c[j].y;
           }
         }
-        if (MODE == MODE_F && zp.L != nullptr) {
+        if (full) {
           T bb = zp.bconst[ii];
-          if (zp.stab != nullptr) {
-            const P2 sv = zp.stab[(long long)ii * zp.nrad + i];
-            bb += sv.x + sv.y * fr;
-          }
+          if (zp.stab != nullptr) bb += sv[ii].x + sv[ii].y * fr;
           t.x -= bb * Lk.x;
           t.y -= bb * Lk.y;
         }
-        buf[ii * N * B + e] = t;
+        if (valid) buf[ii * N * B + e] = t;
       }
     }
   }

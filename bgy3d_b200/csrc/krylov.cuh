@@ -1,0 +1,139 @@
+// krylov.cuh -- Gram-Schmidt kernels of the GMRES driver.
+//
+// Classical Gram-Schmidt needs two passes per Krylov step: h = V^T w (all
+// previous basis vectors against the new one) and w -= V h (with ||w||).
+// Both read the new vector once and up to kVecMax basis vectors in the same
+// sweep, 16-byte vector loads, FP64 accumulation; block partials are summed
+// on the device so only the final coefficients cross to the host.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace rism {
+
+constexpr int kVecMax = 32;
+
+template <typename T> struct VecSet {
+  const T *p[kVecMax];
+};
+struct Coefs {
+  double c[kVecMax];
+};
+
+template <typename T> struct Wide;
+template <> struct Wide<float> { using type = float4; static constexpr int n = 4; };
+template <> struct Wide<double> { using type = double2; static constexpr int n = 2; };
+
+// part[b * kVecMax + v] = sum over block b's range of w . V_v  (v < nv)
+template <typename T>
+__global__ void __launch_bounds__(256) k_mdotv(long long nw, const T *__restrict__ w, int nv, VecSet<T> vs,
+                                              double *__restrict__ part) {
+  using VT = typename Wide<T>::type;
+  constexpr int WN = Wide<T>::n;
+  double acc[kVecMax];
+#pragma unroll
+  for (int v = 0; v < kVecMax; ++v) acc[v] = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += (long long)gridDim.x * blockDim.x) {
+    const VT a = reinterpret_cast<const VT *>(w)[i];
+    const T *ar = reinterpret_cast<const T *>(&a);
+#pragma unroll
+    for (int v = 0; v < kVecMax; ++v) {
+      if (v < nv) {
+        const VT b = reinterpret_cast<const VT *>(vs.p[v])[i];
+        const T *br = reinterpret_cast<const T *>(&b);
+        // products in the basis precision, one conversion per vector load
+        // (float -> double conversions would otherwise bound the kernel)
+        T s = T(0);
+#pragma unroll
+        for (int q = 0; q < WN; ++q) s += ar[q] * br[q];
+        acc[v] += (double)s;
+      }
+    }
+  }
+  __shared__ double sm[kVecMax][8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int v = 0; v < kVecMax; ++v) {
+    if (v < nv) {
+      double a = acc[v];
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+      if (lane == 0) sm[v][wid] = a;
+    }
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < nv) {
+    double a = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) a += sm[threadIdx.x][q];
+    part[(long long)blockIdx.x * kVecMax + threadIdx.x] = a;
+  }
+}
+
+// w = ws * w - sum_v c_v V_v; part[b] = block b's sum of w^2 (if part).
+template <typename T>
+__global__ void __launch_bounds__(256) k_maxpyv(long long nw, T *__restrict__ w, double ws, int nv, VecSet<T> vs,
+                                               Coefs cf, double *__restrict__ part) {
+  using VT = typename Wide<T>::type;
+  constexpr int WN = Wide<T>::n;
+  // the update runs in the basis precision; coefficients converted once
+  T c[kVecMax];
+#pragma unroll
+  for (int v = 0; v < kVecMax; ++v) c[v] = (T)cf.c[v];
+  const T wsT = (T)ws;
+  double s2 = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += (long long)gridDim.x * blockDim.x) {
+    const VT a = reinterpret_cast<const VT *>(w)[i];
+    const T *ar = reinterpret_cast<const T *>(&a);
+    VT o;
+    T *r = reinterpret_cast<T *>(&o);
+#pragma unroll
+    for (int q = 0; q < WN; ++q) r[q] = ws == 0.0 ? T(0) : wsT * ar[q];
+#pragma unroll
+    for (int v = 0; v < kVecMax; ++v) {
+      if (v < nv) {
+        const VT b = reinterpret_cast<const VT *>(vs.p[v])[i];
+        const T *br = reinterpret_cast<const T *>(&b);
+#pragma unroll
+        for (int q = 0; q < WN; ++q) r[q] -= c[v] * br[q];
+      }
+    }
+    T sq = T(0);
+#pragma unroll
+    for (int q = 0; q < WN; ++q) sq += r[q] * r[q];
+    s2 += (double)sq;
+    reinterpret_cast<VT *>(w)[i] = o;
+  }
+  if (part) {
+    for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    __shared__ double sm[8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sm[wid] = s2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0.0;
+      for (int q = 0; q < (int)(blockDim.x >> 5); ++q) a += sm[q];
+      part[blockIdx.x] = a;
+    }
+  }
+}
+
+// out[v] = sum_b part[b * stride + v] for v < nv: one block of kVecMax x 8
+// threads, each summing every 8th partial, then a fixed-order combine.
+__global__ static void __launch_bounds__(kVecMax * 8) k_colsum(int nblk, int stride, int nv,
+                                                              const double *__restrict__ part,
+                                                              double *__restrict__ out) {
+  const int v = threadIdx.x % kVecMax, j = threadIdx.x / kVecMax;
+  __shared__ double sm[8][kVecMax];
+  double a = 0.0;
+  if (v < nv)
+#pragma unroll 4
+    for (int b = j; b < nblk; b += 8) a += part[(long long)b * stride + v];
+  sm[j][v] = a;
+  __syncthreads();
+  if (j == 0 && v < nv) {
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s += sm[q][v];
+    out[v] = s;
+  }
+}
+
+}  // namespace rism

@@ -20,6 +20,7 @@
 
 #include "kernels.cuh"
 #include "kernels_static.cuh"
+#include "krylov.cuh"
 #include "rism3d.h"
 
 using namespace rism;
@@ -149,9 +150,11 @@ struct rism3d_ctx {
 
   NormPartial *npart = nullptr;
   std::vector<NormPartial> h_npart;
-  double *dpart = nullptr;
+  double *dpart = nullptr;       // [red_blocks][kVecMax] reduction partials
+  double *dres = nullptr;        // [kVecMax * 2] reduced coefficients (device)
+  double *hres = nullptr;        // pinned host copy of dres
   std::vector<double> h_dpart;
-  int red_blocks = 1184;
+  int red_blocks = 592;
 
   // solver work (lazily allocated)
   double *F64 = nullptr, *X64t = nullptr, *F64t = nullptr;
@@ -178,7 +181,8 @@ struct rism3d_ctx {
     for (int i = 0; i < 3; ++i) { fr(tw64[i]); fr(tw32[i]); }
     fr(post64); fr(post32); fr(v64); fr(v32); fr(L64); fr(L32);
     fr(chi64); fr(s64); fr(chi32); fr(s32); fr(W); fr(d_solute); fr(d_charge);
-    fr(npart); fr(dpart); fr(F64); fr(X64t); fr(F64t); fr(X32); fr(F32); fr(X32t); fr(F32t);
+    fr(npart); fr(dpart); fr(dres); fr(F64); fr(X64t); fr(F64t); fr(X32); fr(F32); fr(X32t); fr(F32t);
+    if (hres) cudaFreeHost(hres);
     fr(d64); fr(d32); fr(dx64); fr(dx32); fr(d_err);
     for (auto p : basis64) fr(p);
     for (auto p : basis32) fr(p);
@@ -264,8 +268,10 @@ template <typename T> size_t zsmem(rism3d_ctx *c) {
 
 // ---- shape-specialised passes
 constexpr int kStaticRX = 16;
-// y/z tile width: 128-byte rows (16 float2 or 8 double2)
+// y tile width: 128-byte rows (16 float2 or 8 double2); z tile width: 64-byte
+// rows, so the m-site z tile is half as large and four CTAs share an SM
 template <typename T> constexpr int static_B() { return sizeof(T) == 4 ? 16 : 8; }
+template <typename T> constexpr int static_Bz() { return sizeof(T) == 4 ? 8 : 4; }
 template <typename T, int M> constexpr size_t xs_smem() {
   return sizeof(typename Cx<T>::type) * (size_t)(M + kStaticRX * (M + M / Split<M>::R2));
 }
@@ -273,7 +279,7 @@ template <typename T, int N> constexpr size_t ys_smem() {
   return sizeof(typename Cx<T>::type) * (size_t)(N * static_B<T>() + N) + 16;
 }
 template <typename T, int N> size_t zs_smem(int m) {
-  return sizeof(typename Cx<T>::type) * (size_t)(m * N * static_B<T>() + N) + 16;
+  return sizeof(typename Cx<T>::type) * (size_t)(m * N * static_Bz<T>() + N) + 16;
 }
 bool static_len_x(int M) { return M == 48 || M == 64 || M == 128; }
 bool static_len_yz(int N) { return N == 96 || N == 128 || N == 256; }
@@ -343,7 +349,7 @@ template <typename T, int MODE> void launch_z(rism3d_ctx *c) {
   auto *W = c->work<T>();
   const ZParams<T> zp = zparams<T>(c, MODE == MODE_F);
   if (c->stat[sizeof(T) == 8 ? 0 : 1]) {
-    constexpr int B = static_B<T>();
+    constexpr int B = static_Bz<T>();
     dim3 grid((c->g.Nh + B - 1) / B, c->g.N1);
     const CUtensorMap &tm = c->tmz[sizeof(T) == 8 ? 0 : 1];
     const auto *tw = static_cast<const typename Cx<T>::type *>(c->plan<T>(2).tw);
@@ -463,65 +469,58 @@ int vec_grid(long long n) {
 
 template <typename T> VecRef<T> vref(const T *p, double s) { return VecRef<T>{p, s}; }
 
-// h[i] = <w * ws, s_i V_i> for i < nv.
+// h[i] = <w * ws, s_i V_i> for i < nv: one sweep per kVecMax basis vectors,
+// partials summed on the device.
 template <typename T>
 void mdot(rism3d_ctx *c, const T *w, double ws, const std::vector<VecRef<T>> &V, std::vector<double> &h) {
-  TimeScope ts(c, TK_VEC, sizeof(T) == 8 ? 0 : 1, ((int)V.size() + kDotChunk - 1) / kDotChunk);
   const int nv = (int)V.size();
+  const int chunks = (nv + kVecMax - 1) / kVecMax;
+  TimeScope ts(c, TK_VEC, sizeof(T) == 8 ? 0 : 1, 2 * chunks);
   h.assign(nv, 0.0);
   const int G = c->red_blocks;
-  for (int base = 0; base < nv; base += kDotChunk) {
-    VecRef<T> r[kDotChunk];
-    const int k = std::min(kDotChunk, nv - base);
-    for (int i = 0; i < kDotChunk; ++i) r[i] = i < k ? V[base + i] : V[base];
-    k_mdot<T><<<G, 256, 0, c->stream>>>(c->nvec, w, ws, k, r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7],
-                                         c->dpart);
+  const long long nw = c->nvec / Wide<T>::n;
+  for (int base = 0; base < nv; base += kVecMax) {
+    const int k = std::min(kVecMax, nv - base);
+    VecSet<T> vs{};
+    for (int i = 0; i < kVecMax; ++i) vs.p[i] = V[base + (i < k ? i : 0)].p;
+    k_mdotv<T><<<G, 256, 0, c->stream>>>(nw, w, k, vs, c->dpart);
     CKL();
-    c->h_dpart.resize((size_t)G * kDotChunk);
-    CK(cudaMemcpyAsync(c->h_dpart.data(), c->dpart, sizeof(double) * G * kDotChunk, cudaMemcpyDeviceToHost,
-                       c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    for (int b = 0; b < G; ++b)
-      for (int i = 0; i < k; ++i) h[base + i] += c->h_dpart[(size_t)b * kDotChunk + i];
+    k_colsum<<<1, kVecMax * 8, 0, c->stream>>>(G, kVecMax, k, c->dpart, c->dres + base);
+    CKL();
   }
+  CK(cudaMemcpyAsync(c->hres, c->dres, sizeof(double) * nv, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < nv; ++i) h[i] = c->hres[i] * ws * V[i].s;
 }
 
 // w = ws * w - sum_i coef_i (s_i V_i); returns ||w||_2 if want_norm.
 template <typename T>
 double maxpy(rism3d_ctx *c, T *w, double ws, const std::vector<VecRef<T>> &V, const std::vector<double> &coef,
              bool want_norm) {
-  TimeScope ts(c, TK_VEC, sizeof(T) == 8 ? 0 : 1, std::max(1, ((int)V.size() + kDotChunk - 1) / kDotChunk));
   const int nv = (int)V.size();
+  const int chunks = std::max(1, (nv + kVecMax - 1) / kVecMax);
+  TimeScope ts(c, TK_VEC, sizeof(T) == 8 ? 0 : 1, chunks + (want_norm ? 1 : 0));
   const int G = c->red_blocks;
-  double *dcoef = c->dpart + (size_t)G * kDotChunk;  // scratch after the partials
-  double norm = 0.0;
-  if (nv == 0) {
-    VecRef<T> r0 = vref<T>(w, 0.0);
-    k_maxpy<T><<<G, 256, 0, c->stream>>>(c->nvec, w, ws, 0, r0, r0, r0, r0, r0, r0, r0, r0, dcoef,
-                                          want_norm ? c->dpart : nullptr);
+  const long long nw = c->nvec / Wide<T>::n;
+  for (int base = 0; base < std::max(nv, 1); base += kVecMax) {
+    const int k = std::min(kVecMax, nv - base);
+    VecSet<T> vs{};
+    Coefs cf{};
+    for (int i = 0; i < kVecMax; ++i) {
+      vs.p[i] = i < k ? V[base + i].p : w;
+      cf.c[i] = i < k ? coef[base + i] * V[base + i].s : 0.0;
+    }
+    const bool last = base + kVecMax >= nv;
+    k_maxpyv<T><<<G, 256, 0, c->stream>>>(nw, w, base == 0 ? ws : 1.0, std::max(k, 0), vs, cf,
+                                           (last && want_norm) ? c->dpart : nullptr);
     CKL();
   }
-  for (int base = 0; base < nv; base += kDotChunk) {
-    const int k = std::min(kDotChunk, nv - base);
-    VecRef<T> r[kDotChunk];
-    for (int i = 0; i < kDotChunk; ++i) r[i] = i < k ? V[base + i] : V[base];
-    CK(cudaMemcpyAsync(dcoef, coef.data() + base, sizeof(double) * k, cudaMemcpyHostToDevice, c->stream));
-    const bool last = base + kDotChunk >= nv;
-    k_maxpy<T><<<G, 256, 0, c->stream>>>(c->nvec, w, base == 0 ? ws : 1.0, k, r[0], r[1], r[2], r[3], r[4],
-                                          r[5], r[6], r[7], dcoef, (last && want_norm) ? c->dpart : nullptr);
-    CKL();
-  }
-  if (want_norm) {
-    c->h_dpart.resize(G);
-    CK(cudaMemcpyAsync(c->h_dpart.data(), c->dpart, sizeof(double) * G, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    double s = 0.0;
-    for (int b = 0; b < G; ++b) s += c->h_dpart[b];
-    norm = std::sqrt(s);
-  } else {
-    CK(cudaStreamSynchronize(c->stream));  // coef upload buffer is reused
-  }
-  return norm;
+  if (!want_norm) return 0.0;
+  k_colsum<<<1, kVecMax * 8, 0, c->stream>>>(G, 1, 1, c->dpart, c->dres);
+  CKL();
+  CK(cudaMemcpyAsync(c->hres, c->dres, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return std::sqrt(c->hres[0]);
 }
 
 template <typename TX, typename TY> void axpby(rism3d_ctx *c, double a, const TX *x, double b, TY *y) {
@@ -672,7 +671,8 @@ struct NewtonOut {
 // state and residual in TS, Jacobian products and Krylov basis in TJ.
 // Stops when ||F||_inf < tol.
 template <typename TS, typename TJ>
-NewtonOut newton(rism3d_ctx *c, TS *x, double tol, int max_iter, double krylov_rtol, int restart) {
+NewtonOut newton(rism3d_ctx *c, TS *x, double tol, int max_iter, double krylov_rtol, int restart,
+                 double eta0 = 0.5) {
   NewtonOut o;
   TS *F = xbuf<TS>(c, 0);
   TS *xt = xbuf<TS>(c, 1);
@@ -684,6 +684,10 @@ NewtonOut newton(rism3d_ctx *c, TS *x, double tol, int max_iter, double krylov_r
   TJ *rhs = xbuf<TJ>(c, sizeof(TJ) == sizeof(TS) ? 2 : 1);
   double r[2];
   eval_F<TS>(c, x, F, r);
+  // Eisenstat-Walker forcing (PETSc's version 2: gamma 0.9, alpha 2,
+  // safeguard above 0.1), floored at the reference's fixed KSP rtol and
+  // never below what the last step needs to reach tol.
+  double eta = eta0, r2_prev = -1.0;
   for (int it = 0;; ++it) {
     o.rinf = r[0];
     o.r2 = r[1];
@@ -694,10 +698,19 @@ NewtonOut newton(rism3d_ctx *c, TS *x, double tol, int max_iter, double krylov_r
     if (r[0] < tol) { o.converged = true; break; }
     if (it >= max_iter) break;
     o.iters = it + 1;
+    if (r2_prev > 0.0) {
+      const double ratio = r[1] / r2_prev;
+      double e = 0.9 * ratio * ratio;
+      const double guard = 0.9 * eta * eta;
+      if (guard > 0.1) e = std::max(e, guard);
+      eta = std::min(0.9, e);
+    }
+    const double eta_use = std::max(std::max(eta, krylov_rtol), std::min(0.9, 0.5 * tol / r[0]));
+    r2_prev = r[1];
     closure_slope<TS, TJ>(c, x, d);
     axpby<TS, TJ>(c, -1.0, F, 0.0, rhs);
-    const int kits = gmres<TJ>(c, d, rhs, dx, krylov_rtol, 1000, restart);
-    if (c->pd.verbosity > 0) std::fprintf(stderr, "   gmres: %d J.v\n", kits);
+    const int kits = gmres<TJ>(c, d, rhs, dx, eta_use, 1000, restart);
+    if (c->pd.verbosity > 0) std::fprintf(stderr, "   gmres: %d J.v (rtol %.2e)\n", kits, eta_use);
     const double f0 = r[1] * r[1];
     double lam = 1.0, f1 = 0.0, rt[2] = {0, 0};
     bool decreased = false;
@@ -769,7 +782,7 @@ int solve_impl(rism3d_ctx *c, double *T, rism3d_result *out) {
       NewtonOut a = newton<float, float>(c, c->X32, tol32, pd.max_iter, krtol, restart);
       axpby<float, double>(c, 1.0, c->X32, 0.0, T);
       // FP64 residual with FP32 Jacobian: iterative refinement to norm_tol.
-      o = newton<double, float>(c, T, pd.norm_tol, pd.max_iter, krtol, restart);
+      o = newton<double, float>(c, T, pd.norm_tol, pd.max_iter, krtol, restart, krtol);
       o.iters += a.iters;
     } else {
       o = newton<double, double>(c, T, pd.norm_tol, pd.max_iter, krtol, restart);
@@ -986,7 +999,9 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
     CK(cudaDeviceSynchronize());
     cudaFree(d_solvent);
     CK(cudaMalloc(&c->W, sizeof(double2) * (size_t)(m * G.Nc)));
-    c->dpart = dalloc<double>((size_t)c->red_blocks * kDotChunk + 64);
+    c->dpart = dalloc<double>((size_t)c->red_blocks * kVecMax + 64);
+    c->dres = dalloc<double>(4 * kVecMax);
+    CK(cudaMallocHost(&c->hres, sizeof(double) * 4 * kVecMax));
     const int rows = G.N1 * G.N2;
     const int rxmin = std::min(std::min(c->tiles[0].RX, c->tiles[1].RX), kStaticRX);
     c->npart = dalloc<NormPartial>((size_t)((rows + rxmin - 1) / rxmin) * m);
@@ -998,8 +1013,9 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
     if (static_len_x(G.M) && static_len_yz(G.N1) && static_len_yz(G.N2) && m <= 3 && !(gen && gen[0] == '1')) {
       for (int pr = 0; pr < 2; ++pr) {
         const int B = pr == 0 ? static_B<double>() : static_B<float>();
+        const int Bz = pr == 0 ? static_Bz<double>() : static_Bz<float>();
         make_tmap(c, &c->tmy[pr], pr == 0, B, G.N1, 1);
-        make_tmap(c, &c->tmz[pr], pr == 0, B, 1, G.N2);
+        make_tmap(c, &c->tmz[pr], pr == 0, Bz, 1, G.N2);
         c->stat[pr] = true;
       }
     }
@@ -1060,12 +1076,12 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
   allow((const void *)k_y_s<T, true, 128, static_B<T>()>);                                  \
   allow((const void *)k_y_s<T, false, 256, static_B<T>()>);                                 \
   allow((const void *)k_y_s<T, true, 256, static_B<T>()>);                                  \
-  allow((const void *)k_z_s<T, MODE_F, 96, static_B<T>(), 3>);                              \
-  allow((const void *)k_z_s<T, MODE_J, 96, static_B<T>(), 3>);                              \
-  allow((const void *)k_z_s<T, MODE_F, 128, static_B<T>(), 3>);                             \
-  allow((const void *)k_z_s<T, MODE_J, 128, static_B<T>(), 3>);                             \
-  allow((const void *)k_z_s<T, MODE_F, 256, static_B<T>(), 3>);                             \
-  allow((const void *)k_z_s<T, MODE_J, 256, static_B<T>(), 3>);
+  allow((const void *)k_z_s<T, MODE_F, 96, static_Bz<T>(), 3>);                              \
+  allow((const void *)k_z_s<T, MODE_J, 96, static_Bz<T>(), 3>);                              \
+  allow((const void *)k_z_s<T, MODE_F, 128, static_Bz<T>(), 3>);                             \
+  allow((const void *)k_z_s<T, MODE_J, 128, static_Bz<T>(), 3>);                             \
+  allow((const void *)k_z_s<T, MODE_F, 256, static_Bz<T>(), 3>);                             \
+  allow((const void *)k_z_s<T, MODE_J, 256, static_Bz<T>(), 3>);
       OPTIN_S(double)
       OPTIN_S(float)
 #undef OPTIN_S
