@@ -39,7 +39,9 @@ class Problem(ctypes.Structure):
                 ("closure", ctypes.c_int), ("max_iter", ctypes.c_int),
                 ("norm_tol", ctypes.c_double), ("lambda_", ctypes.c_double),
                 ("solver", ctypes.c_int), ("renorm", ctypes.c_int),
-                ("precision", ctypes.c_int), ("verbosity", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("verbosity", ctypes.c_int),
+                ("krylov_restart", ctypes.c_int), ("ew_forcing", ctypes.c_int),
+                ("coarse_h", ctypes.c_double), ("coarse_steps", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):
@@ -49,7 +51,8 @@ class Result(ctypes.Structure):
                 ("resid_2", ctypes.c_double), ("status", ctypes.c_int),
                 ("newton_iters", ctypes.c_int), ("f_evals", ctypes.c_int),
                 ("jv_evals", ctypes.c_int), ("f_evals_fp32", ctypes.c_int),
-                ("jv_evals_fp32", ctypes.c_int), ("seconds", ctypes.c_double)]
+                ("jv_evals_fp32", ctypes.c_int), ("jv_evals_coarse", ctypes.c_int),
+                ("seconds", ctypes.c_double)]
 
 
 # Every entry point declared in include/rism3d.h (checked by the CPU tests).
@@ -59,6 +62,7 @@ EXPORTS = [
     "rism3d_jacobian_t1", "rism3d_iterate_t1_f32", "rism3d_jacobian_t1_f32",
     "rism3d_solve", "rism3d_observables", "rism3d_get_field", "rism3d_last_error",
     "rism3d_profile", "rism1d_solvent_chi", "rism3d_jacobian_apply_noalloc",
+    "rism3d_precondition", "rism3d_coarse_grid",
 ]
 
 _lib = None
@@ -103,6 +107,10 @@ def lib():
     L.rism1d_solvent_chi.restype = I
     L.rism3d_jacobian_apply_noalloc.argtypes = [P(Problem), I, P(D), V, V, V]
     L.rism3d_jacobian_apply_noalloc.restype = I
+    L.rism3d_precondition.argtypes = [V, V, V, V]
+    L.rism3d_precondition.restype = I
+    L.rism3d_coarse_grid.argtypes = [V, P(I)]
+    L.rism3d_coarse_grid.restype = I
     _lib = L
     return L
 

@@ -22,6 +22,7 @@
 #include "kernels_static.cuh"
 #include "krylov.cuh"
 #include "rism3d.h"
+#include "twogrid.cuh"
 
 using namespace rism;
 
@@ -118,8 +119,8 @@ struct TileShape {
 struct PassTimer {
   bool on = false;
   cudaEvent_t a, b;
-  double ms[10] = {0};
-  long long launches[10] = {0};
+  double ms[12] = {0};
+  long long launches[12] = {0};
 };
 
 struct rism3d_ctx {
@@ -165,6 +166,18 @@ struct rism3d_ctx {
   std::vector<float *> basis32;
   double *dx64 = nullptr;
   float *dx32 = nullptr;
+  std::vector<double *> zbasis64;  // flexible-GMRES preconditioned directions
+  std::vector<float *> zbasis32;
+
+  // two-grid preconditioner: the coarse problem and the per-axis transfer
+  // matrices R [Nc][N], Rt [N][Nc], P [N][Nc], Pt [Nc][N] (FP32)
+  rism3d_ctx *coarse = nullptr;
+  int Nc[3] = {0, 0, 0};
+  float *tR[3] = {nullptr, nullptr, nullptr}, *tRt[3] = {nullptr, nullptr, nullptr};
+  float *tP[3] = {nullptr, nullptr, nullptr}, *tPt[3] = {nullptr, nullptr, nullptr};
+  float *tA = nullptr, *tB = nullptr;       // partially transferred fields
+  float *tc_r = nullptr, *tc_y = nullptr;   // coarse right-hand side / solution
+  int coarse_jv = 0;
 
   cudaStream_t stream = 0;
   PassTimer timer;
@@ -186,6 +199,11 @@ struct rism3d_ctx {
     fr(d64); fr(d32); fr(dx64); fr(dx32); fr(d_err);
     for (auto p : basis64) fr(p);
     for (auto p : basis32) fr(p);
+    for (auto p : zbasis64) fr(p);
+    for (auto p : zbasis32) fr(p);
+    for (int a = 0; a < 3; ++a) { fr(tR[a]); fr(tRt[a]); fr(tP[a]); fr(tPt[a]); }
+    fr(tA); fr(tB); fr(tc_r); fr(tc_y);
+    delete coarse;
     if (timer.on) { cudaEventDestroy(timer.a); cudaEventDestroy(timer.b); }
   }
 
@@ -199,14 +217,14 @@ template <> const AxisPlan &rism3d_ctx::plan<float>(int a) const { return a == 0
 
 namespace {
 
-enum { TK_XFWD = 0, TK_Y = 1, TK_Z = 2, TK_XINV = 3, TK_VEC = 4 };
+enum { TK_XFWD = 0, TK_Y = 1, TK_Z = 2, TK_XINV = 3, TK_VEC = 4, TK_PREC = 5 };
 
-// Times one pass (when enabled) into bucket which + 5 * precision and
+// Times one pass (when enabled) into bucket which + 6 * precision and
 // always counts its kernel launches.
 struct TimeScope {
   rism3d_ctx *c;
   int which;
-  TimeScope(rism3d_ctx *c_, int w, int prec, int nlaunch = 1) : c(c_), which(w + 5 * prec) {
+  TimeScope(rism3d_ctx *c_, int w, int prec, int nlaunch = 1) : c(c_), which(w + 6 * prec) {
     c->timer.launches[which] += nlaunch;
     if (c->timer.on) cudaEventRecord(c->timer.a, c->stream);
   }
@@ -659,6 +677,161 @@ template <typename TS, typename TJ> void closure_slope(rism3d_ctx *c, const TS *
   CKL();
 }
 
+// ------------------------------------------------ two-grid preconditioner
+// M^-1 v = P (J_H^-1 + I) R v - v.  The slow modes of J = (chi-1)*(c' .) - 1
+// are long-wavelength fields confined to the solute core, where c' -> -1
+// and J -> -chi, whose charge branch vanishes as k -> 0; a coarse problem
+// on the same box at about 1 A spacing resolves them, and everywhere else
+// (c' = 0, or wavelengths the coarse grid does not hold) J is close to -1.
+// R and P are the band-limited transfers of twogrid.cuh.  J_H takes its
+// slope from the fine one, c'_H = R c': exp(-beta v + R t) on the coarse
+// points would overshoot the fine slope many times over in the attractive
+// shells of an unconverged HNC state and wreck the preconditioner there.
+// J_H^-1 is a fixed number of FP32 GMRES steps on the coarse context, so M
+// varies slightly from call to call and the outer solver is flexible GMRES.
+
+long long launch_total(const rism3d_ctx *c) {
+  long long s = 0;
+  for (long long l : c->timer.launches) s += l;
+  return s;
+}
+
+void transfer_axis(rism3d_ctx *c, int outer, int n_in, int n_out, int inner, const float *in, const float *A,
+                   float *out) {
+  const long long tot = (long long)outer * inner;
+  dim3 g((unsigned)((tot + tg::kAxThreads - 1) / tg::kAxThreads), (unsigned)((n_out + tg::kAxJ - 1) / tg::kAxJ));
+  tg::k_transfer_axis<<<g, tg::kAxThreads, 0, c->stream>>>(outer, n_in, n_out, inner, in, A, out);
+  CKL();
+}
+
+// out (coarse [m][Nc2][Nc1][Nc0]) = R (s in), in fine [m][N2][N1][N0].
+template <typename T> void tg_restrict(rism3d_ctx *c, const T *in, double s, float *out) {
+  const Geo &G = c->g;
+  const long long rows = (long long)c->m * G.N2 * G.N1;
+  dim3 gx((unsigned)((rows + tg::kRxRows - 1) / tg::kRxRows), (unsigned)((c->Nc[0] + tg::kRxCols - 1) / tg::kRxCols));
+  tg::k_restrict_x<T><<<gx, tg::kRxThreads, 0, c->stream>>>(rows, G.N0, c->Nc[0], in, (float)s, c->tRt[0], c->tA);
+  CKL();
+  transfer_axis(c, c->m * G.N2, G.N1, c->Nc[1], c->Nc[0], c->tA, c->tR[1], c->tB);
+  transfer_axis(c, c->m, G.N2, c->Nc[2], c->Nc[1] * c->Nc[0], c->tB, c->tR[2], out);
+}
+
+// out = P yc - s r (fine), yc coarse.
+template <typename T> void tg_prolong(rism3d_ctx *c, const float *yc, const T *r, double s, T *out) {
+  const Geo &G = c->g;
+  transfer_axis(c, c->m, c->Nc[2], G.N2, c->Nc[1] * c->Nc[0], yc, c->tP[2], c->tB);
+  transfer_axis(c, c->m * G.N2, c->Nc[1], G.N1, c->Nc[0], c->tB, c->tP[1], c->tA);
+  const long long rows = (long long)c->m * G.N2 * G.N1;
+  dim3 gx((unsigned)((rows + tg::kPxRows - 1) / tg::kPxRows), (unsigned)((G.N0 + tg::kPxCols - 1) / tg::kPxCols));
+  tg::k_prolong_x<T, T><<<gx, tg::kPxThreads, 0, c->stream>>>(rows, G.N0, c->Nc[0], c->tA, c->tPt[0], r, s, out);
+  CKL();
+}
+
+// Coarse Jacobian of the current Newton step: c'_H = R d, d = c'(t) fine.
+template <typename T> void tg_prepare(rism3d_ctx *c, const T *d) {
+  TimeScope ts(c, TK_PREC, sizeof(T) == 8 ? 0 : 1, 3);
+  tg_restrict<T>(c, d, 1.0, slopebuf<float>(c->coarse));
+}
+
+// z = M^-1 (s v).
+template <typename T> void tg_apply(rism3d_ctx *c, const T *v, double s, T *z) {
+  rism3d_ctx *cc = c->coarse;
+  const int prec = sizeof(T) == 8 ? 0 : 1;
+  const long long l0 = launch_total(cc);
+  {
+    TimeScope ts(c, TK_PREC, prec, 6);
+    tg_restrict<T>(c, v, s, c->tc_r);
+    const int k = c->pd.coarse_steps > 0 ? std::min(c->pd.coarse_steps, 100) : 12;
+    const int jv0 = cc->jv32_evals;
+    gmres<float>(cc, slopebuf<float>(cc), c->tc_r, c->tc_y, 0.0, k, k);
+    c->coarse_jv += cc->jv32_evals - jv0;
+    axpby<float, float>(cc, 1.0, c->tc_r, 1.0, c->tc_y);
+    tg_prolong<T>(c, c->tc_y, v, s, z);
+  }
+  c->timer.launches[TK_PREC + 6 * prec] += launch_total(cc) - l0;
+}
+
+template <typename T> std::vector<T *> &zbasis(rism3d_ctx *c);
+template <> std::vector<double *> &zbasis<double>(rism3d_ctx *c) { return c->zbasis64; }
+template <> std::vector<float *> &zbasis<float>(rism3d_ctx *c) { return c->zbasis32; }
+
+// Flexible GMRES(restart) for J x = b from x0 = 0, right-preconditioned by
+// the two-grid M (z_j = M^-1 v_j, x = sum y_j z_j; Saad, SIAM J. Sci.
+// Comput. 14 (1993) 461).  Classical Gram-Schmidt as in gmres(); returns
+// the number of fine J.v products.
+template <typename T>
+int fgmres(rism3d_ctx *c, const T *d, T *b, T *x, double rtol, int maxit, int restart) {
+  auto &B = basis<T>(c);
+  auto &Z = zbasis<T>(c);
+  ensure_basis<T>(c, 1);
+  std::vector<double> H((size_t)(restart + 1) * restart), cs(restart), sn(restart), gv(restart + 1);
+  std::vector<VecRef<T>> V;
+  std::vector<double> h;
+  bool have_x = false;
+  double beta0 = -1.0;
+  int its = 0;
+  while (its < maxit) {
+    if (!have_x) {
+      axpby<T, T>(c, 1.0, b, 0.0, B[0]);
+    } else {
+      eval_J<T>(c, d, x, 1.0, B[0], nullptr);  // B0 = J x
+      its++;
+      xpay<T, T, T>(c, b, -1.0, B[0], B[0]);   // B0 = b - J x
+    }
+    const double beta = maxpy<T>(c, B[0], 1.0, {}, {}, true);
+    if (beta0 < 0) beta0 = beta;
+    if (beta == 0.0 || beta <= rtol * beta0) break;
+    V.assign(1, vref<T>(B[0], 1.0 / beta));
+    std::fill(gv.begin(), gv.end(), 0.0);
+    gv[0] = beta;
+    int j = 0;
+    bool done = false;
+    for (; j < restart && its < maxit; ++j) {
+      ensure_basis<T>(c, j + 2);
+      while ((int)Z.size() <= j) Z.push_back(dalloc<T>(c->nvec));
+      tg_apply<T>(c, V[j].p, V[j].s, Z[j]);
+      eval_J<T>(c, d, Z[j], 1.0, B[j + 1], nullptr);
+      its++;
+      mdot<T>(c, B[j + 1], 1.0, V, h);
+      const double hn = maxpy<T>(c, B[j + 1], 1.0, V, h, true);
+      for (int i = 0; i <= j; ++i) H[(size_t)i * restart + j] = h[i];
+      H[(size_t)(j + 1) * restart + j] = hn;
+      for (int i = 0; i < j; ++i) {
+        const double a = H[(size_t)i * restart + j], bb = H[(size_t)(i + 1) * restart + j];
+        H[(size_t)i * restart + j] = cs[i] * a + sn[i] * bb;
+        H[(size_t)(i + 1) * restart + j] = -sn[i] * a + cs[i] * bb;
+      }
+      const double a = H[(size_t)j * restart + j], bb = H[(size_t)(j + 1) * restart + j];
+      const double r = std::hypot(a, bb);
+      cs[j] = r == 0.0 ? 1.0 : a / r;
+      sn[j] = r == 0.0 ? 0.0 : bb / r;
+      H[(size_t)j * restart + j] = r;
+      H[(size_t)(j + 1) * restart + j] = 0.0;
+      gv[j + 1] = -sn[j] * gv[j];
+      gv[j] = cs[j] * gv[j];
+      V.push_back(vref<T>(B[j + 1], hn > 0.0 ? 1.0 / hn : 0.0));
+      if (std::fabs(gv[j + 1]) <= rtol * beta0 || hn == 0.0) { ++j; done = true; break; }
+    }
+    const int k = j;
+    std::vector<double> y(k);
+    for (int i = k - 1; i >= 0; --i) {
+      double s = gv[i];
+      for (int l = i + 1; l < k; ++l) s -= H[(size_t)i * restart + l] * y[l];
+      y[i] = H[(size_t)i * restart + i] != 0.0 ? s / H[(size_t)i * restart + i] : 0.0;
+    }
+    std::vector<VecRef<T>> Zk;
+    std::vector<double> my(k);
+    for (int i = 0; i < k; ++i) {
+      Zk.push_back(vref<T>(Z[i], 1.0));
+      my[i] = -y[i];
+    }
+    maxpy<T>(c, x, have_x ? 1.0 : 0.0, Zk, my, false);
+    have_x = true;
+    if (done) break;
+  }
+  if (!have_x) axpby<T, T>(c, 0.0, b, 0.0, x);
+  return its;
+}
+
 struct NewtonOut {
   int iters = 0;
   double rinf = 0, r2 = 0;
@@ -705,11 +878,24 @@ NewtonOut newton(rism3d_ctx *c, TS *x, double tol, int max_iter, double krylov_r
       if (guard > 0.1) e = std::max(e, guard);
       eta = std::min(0.9, e);
     }
-    const double eta_use = std::max(std::max(eta, krylov_rtol), std::min(0.9, 0.5 * tol / r[0]));
+    double eta_use = c->pd.ew_forcing ? std::max(std::max(eta, krylov_rtol), std::min(0.9, 0.5 * tol / r[0]))
+                                      : krylov_rtol;
+    // With the two-grid preconditioner a loose forcing term is met after one
+    // or two iterations by a direction taken mostly from the coarse
+    // Jacobian, which far from the root of an HNC problem can be a poor
+    // descent direction (the line search then creeps).  Preconditioned
+    // iterations are cheap, so those solves are held to 0.1.
+    if (c->coarse) eta_use = std::min(eta_use, 0.1);
     r2_prev = r[1];
     closure_slope<TS, TJ>(c, x, d);
     axpby<TS, TJ>(c, -1.0, F, 0.0, rhs);
-    const int kits = gmres<TJ>(c, d, rhs, dx, eta_use, 1000, restart);
+    int kits;
+    if (c->coarse) {
+      tg_prepare<TJ>(c, d);
+      kits = fgmres<TJ>(c, d, rhs, dx, eta_use, 1000, restart);
+    } else {
+      kits = gmres<TJ>(c, d, rhs, dx, eta_use, 1000, restart);
+    }
     if (c->pd.verbosity > 0) std::fprintf(stderr, "   gmres: %d J.v (rtol %.2e)\n", kits, eta_use);
     const double f0 = r[1] * r[1];
     double lam = 1.0, f1 = 0.0, rt[2] = {0, 0};
@@ -744,12 +930,13 @@ double now_s() {
 int solve_impl(rism3d_ctx *c, double *T, rism3d_result *out) {
   rism3d_result res{};
   c->f_evals = c->jv_evals = c->f32_evals = c->jv32_evals = 0;
+  c->coarse_jv = 0;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   CK(cudaEventRecord(e0, c->stream));
   const double krtol = 1e-3;  // 100 * PETSc default rtol 1e-5 (bgy3d-snes.c:277)
-  const int restart = 30;
+  const int restart = c->pd.krylov_restart > 0 ? std::min(c->pd.krylov_restart, 200) : 30;
   NewtonOut o;
   int status = RISM3D_OK;
   const rism3d_problem &pd = c->pd;
@@ -804,6 +991,7 @@ int solve_impl(rism3d_ctx *c, double *T, rism3d_result *out) {
   res.jv_evals = c->jv_evals;
   res.f_evals_fp32 = c->f32_evals;
   res.jv_evals_fp32 = c->jv32_evals;
+  res.jv_evals_coarse = c->coarse_jv;
   res.seconds = ms * 1e-3;
   if (out) {
     const double keep[5] = {out->mu, out->mu_hnc, out->mu_kh, out->mu_gf, out->pmv_factor};
@@ -1086,6 +1274,52 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
       OPTIN_S(float)
 #undef OPTIN_S
     }
+    // two-grid preconditioner: a copy of the problem on a grid of about
+    // coarse_h spacing, used when that grid is coarser along every axis
+    if (pd->coarse_h > 0 && pd->solver != RISM3D_PICARD) {
+      int nc[3];
+      bool coarser = true;
+      for (int a = 0; a < 3; ++a) {
+        int nn = std::max(8, (int)std::ceil(pd->L[a] / pd->coarse_h - 1e-9));
+        while (!(is_2a3b(nn) && nn % 2 == 0)) ++nn;
+        nc[a] = nn;
+        if (nn >= pd->N[a]) coarser = false;
+      }
+      if (coarser) {
+        rism3d_problem pc = *pd;
+        for (int a = 0; a < 3; ++a) pc.N[a] = nc[a];
+        pc.coarse_h = 0;
+        pc.verbosity = 0;
+        create_impl(&pc, m, solvent, n, solute, chi, &c->coarse);
+        for (int a = 0; a < 3; ++a) {
+          const int nf = pd->N[a], ncs = nc[a];
+          c->Nc[a] = ncs;
+          std::vector<float> R((size_t)ncs * nf), Rt((size_t)nf * ncs), P((size_t)nf * ncs), Pt((size_t)ncs * nf);
+          for (int i = 0; i < ncs; ++i)
+            for (int j = 0; j < nf; ++j) {
+              const double x = (double)i / ncs - (double)j / nf;
+              double s = 0.0;
+              for (int k = -ncs / 2; k <= ncs / 2; ++k)
+                s += (2 * std::abs(k) == ncs ? 0.5 : 1.0) * std::cos(2.0 * pi * k * x);
+              R[(size_t)i * nf + j] = Rt[(size_t)j * ncs + i] = (float)(s / nf);
+              P[(size_t)j * ncs + i] = Pt[(size_t)i * nf + j] = (float)(s / ncs);
+            }
+          auto up = [&](const std::vector<float> &h) {
+            float *dptr = dalloc<float>(h.size());
+            CK(cudaMemcpy(dptr, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice));
+            return dptr;
+          };
+          c->tR[a] = up(R);
+          c->tRt[a] = up(Rt);
+          c->tP[a] = up(P);
+          c->tPt[a] = up(Pt);
+        }
+        c->tA = dalloc<float>((size_t)m * G.N2 * G.N1 * c->Nc[0]);
+        c->tB = dalloc<float>((size_t)m * G.N2 * c->Nc[1] * c->Nc[0]);
+        c->tc_r = dalloc<float>(c->coarse->nvec);
+        c->tc_y = dalloc<float>(c->coarse->nvec);
+      }
+    }
   } catch (...) {
     delete c;
     throw;
@@ -1131,6 +1365,10 @@ void rism3d_problem_defaults(rism3d_problem *pd, double L_half, int N) {
   pd->renorm = 1;
   pd->precision = RISM3D_FP64;
   pd->verbosity = 0;
+  pd->krylov_restart = 30;
+  pd->ew_forcing = 1;
+  pd->coarse_h = 1.0;
+  pd->coarse_steps = 12;
 }
 
 const char *rism3d_last_error(void) { return g_last_error.c_str(); }
@@ -1248,14 +1486,33 @@ int rism3d_solute_solve(const rism3d_problem *pd, int m, const rism3d_site *solv
   return rc;
 }
 
+int rism3d_precondition(rism3d_ctx *ctx, const double *T, const double *v, double *z) {
+  if (!ctx || !T || !v || !z) return RISM3D_ERR_ARG;
+  if (!ctx->coarse) return RISM3D_ERR_UNSUPPORTED;
+  return guard([&] {
+    double *d = slopebuf<double>(ctx);
+    closure_slope<double, double>(ctx, T, d);
+    tg_prepare<double>(ctx, d);
+    tg_apply<double>(ctx, v, 1.0, z);
+    CK(cudaStreamSynchronize(ctx->stream));
+    return (int)RISM3D_OK;
+  });
+}
+
+int rism3d_coarse_grid(rism3d_ctx *ctx, int *n) {
+  if (!ctx || !n) return RISM3D_ERR_ARG;
+  for (int a = 0; a < 3; ++a) n[a] = ctx->coarse ? ctx->Nc[a] : 0;
+  return RISM3D_OK;
+}
+
 // ---- profiling hooks (per-pass CUDA-event timing, off by default) -------
 int rism3d_profile(rism3d_ctx *ctx, int on, double *ms_out, long long *launches_out) {
   if (!ctx) return RISM3D_ERR_ARG;
   return guard([&] {
     if (ms_out)
-      for (int i = 0; i < 10; ++i) ms_out[i] = ctx->timer.ms[i];
+      for (int i = 0; i < 12; ++i) ms_out[i] = ctx->timer.ms[i];
     if (launches_out)
-      for (int i = 0; i < 10; ++i) launches_out[i] = ctx->timer.launches[i];
+      for (int i = 0; i < 12; ++i) launches_out[i] = ctx->timer.launches[i];
     if (on && !ctx->timer.on) {
       CK(cudaEventCreate(&ctx->timer.a));
       CK(cudaEventCreate(&ctx->timer.b));
@@ -1265,7 +1522,7 @@ int rism3d_profile(rism3d_ctx *ctx, int on, double *ms_out, long long *launches_
       cudaEventDestroy(ctx->timer.b);
       ctx->timer.on = false;
     }
-    for (int i = 0; i < 10; ++i) ctx->timer.ms[i] = 0, ctx->timer.launches[i] = 0;
+    for (int i = 0; i < 12; ++i) ctx->timer.ms[i] = 0, ctx->timer.launches[i] = 0;
     return (int)RISM3D_OK;
   });
 }

@@ -24,6 +24,11 @@ DEFAULTS = {
     "L": 10.0, "N": 64, "rho": 0.033427745, "beta": 1.6889, "norm-tol": 1.0e-7,
     "max-iter": 1500, "lambda": 0.02, "closure": "HNC", "snes-solver": "newton",
     "no-renorm": False, "precision": "fp64", "verbosity": 0,
+    # Krylov solver of the Newton steps: restart length, Eisenstat-Walker
+    # forcing (0: the reference's fixed rtol 1e-3), the two-grid
+    # preconditioner's coarse spacing in A (0: off, the reference's
+    # unpreconditioned GMRES) and its coarse GMRES steps.
+    "krylov-restart": 30, "ew-forcing": 1, "coarse-h": 1.0, "coarse-steps": 12,
 }
 
 
@@ -55,6 +60,10 @@ def problem_data(settings):
     pd.renorm = 0 if s["no-renorm"] else 1
     pd.precision = {"fp64": _abi.FP64, "mixed": _abi.MIXED}[s["precision"]]
     pd.verbosity = int(s["verbosity"])
+    pd.krylov_restart = int(s["krylov-restart"])
+    pd.ew_forcing = int(s["ew-forcing"])
+    pd.coarse_h = float(s["coarse-h"])
+    pd.coarse_steps = int(s["coarse-steps"])
     return pd
 
 
@@ -80,6 +89,7 @@ def _result_dict(r):
         "partial-molar-volume-factor": r.pmv_factor, "resid-inf": r.resid_inf, "resid-2": r.resid_2,
         "status": r.status, "newton-iters": r.newton_iters, "f-evals": r.f_evals,
         "jv-evals": r.jv_evals, "f-evals-fp32": r.f_evals_fp32, "jv-evals-fp32": r.jv_evals_fp32,
+        "jv-evals-coarse": r.jv_evals_coarse,
         "seconds": r.seconds,
     }
 
@@ -204,6 +214,22 @@ class RismContext:
                       self._check_vec(out, T.dtype)), "jacobian_t1")
         return out
 
+    def coarse_grid(self):
+        """Points per axis of the two-grid preconditioner's coarse grid
+        (None when it is off)."""
+        n = (ctypes.c_int * 3)()
+        _abi.check(_abi.lib().rism3d_coarse_grid(self._h, n), "coarse_grid")
+        return None if n[0] == 0 else (n[0], n[1], n[2])
+
+    def precondition(self, T, v, out=None):
+        """Two-grid preconditioner at state T: M^-1 v (FP64 device tensors)."""
+        t = self._torch
+        out = t.empty_like(v) if out is None else out
+        _abi.check(_abi.lib().rism3d_precondition(self._h, self._check_vec(T, t.float64),
+                                                  self._check_vec(v, t.float64),
+                                                  self._check_vec(out, t.float64)), "precondition")
+        return out
+
     def solve(self, T=None):
         """Newton solve in place on a device FP64 tensor; returns (T, result dict)."""
         T = self.zeros() if T is None else T
@@ -232,11 +258,12 @@ class RismContext:
 
     def profile(self, on=True):
         """Enable/disable per-pass event timing; returns and resets the totals
-        {(pass, precision): (ms, launches)}, pass in xfwd/y/z/xinv/vec and
+        {(pass, precision): (ms, launches)}, pass in xfwd/y/z/xinv/vec/prec
+        (prec: the two-grid preconditioner, its coarse solve included) and
         precision in f64/f32 (launches are counted with timing off too)."""
-        ms = (ctypes.c_double * 10)()
-        ln = (ctypes.c_longlong * 10)()
+        ms = (ctypes.c_double * 12)()
+        ln = (ctypes.c_longlong * 12)()
         _abi.check(_abi.lib().rism3d_profile(self._h, 1 if on else 0, ms, ln), "profile")
-        names = ["xfwd", "y", "z", "xinv", "vec"]
-        return {(k, p): (ms[i + 5 * j], ln[i + 5 * j]) for j, p in enumerate(("f64", "f32"))
+        names = ["xfwd", "y", "z", "xinv", "vec", "prec"]
+        return {(k, p): (ms[i + 6 * j], ln[i + 6 * j]) for j, p in enumerate(("f64", "f32"))
                 for i, k in enumerate(names)}

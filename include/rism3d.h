@@ -83,6 +83,19 @@ typedef struct rism3d_problem {
   int renorm;         /* 1: default; 0: --no-renorm (hnc3d.c:1607-1615) */
   int precision;      /* RISM3D_FP64 or RISM3D_MIXED */
   int verbosity;      /* 0 silent; 1 one line per Newton step on stderr */
+  /* Krylov solver of the Newton steps.  krylov_restart 30, ew_forcing 0 and
+     coarse_h 0 are the reference's settings: GMRES(30) without
+     preconditioner at a fixed KSP rtol of 1e-3 (bgy3d-snes.c:262-306).
+     rism3d_problem_defaults() selects 30 / 1 / 1.0 / 12. */
+  int krylov_restart; /* GMRES restart length (0: 30) */
+  int ew_forcing;     /* 1: Eisenstat-Walker forcing terms, floored at 1e-3;
+                         0: fixed rtol 1e-3 */
+  double coarse_h;    /* two-grid preconditioner (then flexible GMRES):
+                         coarse grid spacing in A -- per axis the smallest
+                         even 2^a 3^b point count n with L / n <= coarse_h;
+                         off when 0 or when that grid is not coarser than N
+                         along every axis */
+  int coarse_steps;   /* GMRES steps of each coarse solve (0: 12) */
 } rism3d_problem;
 
 /* What hnc3d_solute_solve conses onto its result alist
@@ -98,6 +111,7 @@ typedef struct rism3d_result {
   int f_evals;        /* F evaluations (iterate_t1), all precisions */
   int jv_evals;       /* J.v products (jacobian_t1), all precisions */
   int f_evals_fp32, jv_evals_fp32;
+  int jv_evals_coarse; /* J.v products on the coarse grid (preconditioner) */
   double seconds;     /* device time of the non-linear solve */
 } rism3d_result;
 
@@ -174,12 +188,27 @@ int rism3d_get_field(rism3d_ctx *ctx, int which, double *dst);
 /* Last CUDA error string of this thread (diagnostics). */
 const char *rism3d_last_error(void);
 
+/* The two-grid preconditioner of the Newton-Krylov solver at state T
+   (diagnostics and tests; the reference's GMRES has no preconditioner, so
+   this has no counterpart there): z = M^-1 v with
+   M^-1 v = P (J_H^-1 + I) R v - v, where R / P are the band-limited
+   transfers to / from the coarse grid, J_H the coarse Jacobian built from
+   the restricted closure slope R c'(T), and J_H^-1 a coarse_steps-step
+   FP32 GMRES from zero.  Device pointers, FP64 [m][N2][N1][N0].  Returns
+   RISM3D_ERR_UNSUPPORTED when the context has no coarse grid. */
+int rism3d_precondition(rism3d_ctx *ctx, const double *T, const double *v, double *z);
+
+/* Points per axis of the two-grid preconditioner's coarse grid, written to
+   n[3] (zeros when the preconditioner is off). */
+int rism3d_coarse_grid(rism3d_ctx *ctx, int *n);
+
 /* Per-pass CUDA-event timing (diagnostics): on != 0 enables it (it
    synchronises after every pass, so it is for measurement only).  The
-   totals accumulated since the last call are returned in ms[10] /
-   launches[10] (either may be NULL) and reset; bucket = pass + 5 * p with
-   pass 0..4 = x-forward, y, z, x-inverse, vector ops and p = 0 for FP64,
-   1 for FP32.  Launches are counted even when timing is off. */
+   totals accumulated since the last call are returned in ms[12] /
+   launches[12] (either may be NULL) and reset; bucket = pass + 6 * p with
+   pass 0..5 = x-forward, y, z, x-inverse, vector ops, two-grid
+   preconditioner (grid transfers and the whole coarse solve) and p = 0
+   for FP64, 1 for FP32.  Launches are counted even when timing is off. */
 int rism3d_profile(rism3d_ctx *ctx, int on, double *ms, long long *launches);
 
 /* Jacobian product J dT = (chi - 1) * (d . dT) - dT for a caller-supplied

@@ -186,6 +186,18 @@ def test_readme_water_96(fixture_loader):
         assert round(out["free-energy"], 6) == -6.349052
 
 
+@pytest.mark.parametrize("opts", [{"coarse-h": 0, "ew-forcing": 0}, {"coarse-h": 0}, {"krylov-restart": 8},
+                                  {"coarse-steps": 4, "precision": "mixed"}])
+def test_krylov_options_reach_the_same_root(fixture_loader, opts):
+    """The Krylov options change the path to the root, never the root."""
+    meta, arr = fixture_loader("synth6_kh_n32")
+    out = hnc3d_run_solute(meta["solute"], meta["solvent"],
+                           settings_of(meta, **{"norm-tol": 1e-12, **opts}), arr["chi"])
+    assert out["resid-inf"] < 1e-12
+    assert abs(out["free-energy"] - meta["mu"]) < 1e-6
+    assert np.max(np.abs(out["RESTART"] - arr["T"])) < 1e-10
+
+
 def test_picard_and_trial_solvers(fixture_loader):
     meta, arr = fixture_loader("water_hnc_n24")
     for solver in ("trial",):

@@ -1,0 +1,127 @@
+"""Two-grid preconditioner of the Newton-Krylov solver (sm_100a path).
+
+M^-1 v = P (J_H^-1 + I) R v - v with band-limited transfers R / P, the
+coarse Jacobian J_H built from the restricted closure slope R c'(T), and a
+fixed-step GMRES for J_H^-1.  The GPU result is checked against a NumPy
+restatement on the oracle's operators at the coarse size; the coarse solve
+runs in FP32 on the GPU, so the tolerance is 1e-4 of max|z|.  The
+runtime-length FFT passes at the coarse sizes (16^3, 18^3, 48^3) are
+checked against the oracle at the usual 1e-11 (FP64) / 2e-5 (FP32), and
+solves with the preconditioner on, started from zero, reach the oracle's
+root.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+from bgy3d_b200 import RismContext, hnc3d_run_solute  # noqa: E402
+from oracle import closures as cl  # noqa: E402
+from oracle import hnc3d  # noqa: E402
+
+
+def settings_of(meta, **kw):
+    s = dict(meta["settings"])
+    s["closure"] = int(s["closure"])
+    s.update(kw)
+    return s
+
+
+def problem(meta, chi, n):
+    s = meta["settings"]
+    return hnc3d.Problem((n,) * 3, (2 * s["L"],) * 3, s["beta"], s["rho"], int(s["closure"]), meta["solvent"],
+                         meta["solute"], chi, s["rmax"], renorm=not s["no-renorm"])
+
+
+def to_dev(a, dtype=torch.float64):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(device="cuda", dtype=dtype)
+
+
+def transfer(n, nc):
+    """R [nc][n] and P [n][nc]: keep the modes |k| <= nc/2 (half weight at nc/2)."""
+    x = np.arange(nc)[:, None] / nc - np.arange(n)[None, :] / n
+    S = sum((0.5 if 2 * abs(k) == nc else 1.0) * np.cos(2 * np.pi * k * x) for k in range(-nc // 2, nc // 2 + 1))
+    return S / n, (S / nc).T
+
+
+def along(A, f):
+    """Apply A along the three grid axes of f [m][z][y][x]."""
+    f = np.einsum("ai,mzyi->mzya", A, f)
+    f = np.einsum("ai,mziy->mzay", A, f)
+    return np.einsum("ai,mizy->mazy", A, f)
+
+
+def gmres_steps(A, b, k):
+    """k steps of GMRES from 0 (classical Gram-Schmidt): the coarse solve."""
+    beta = np.linalg.norm(b)
+    V = [b / beta]
+    H = np.zeros((k + 1, k))
+    for j in range(k):
+        w = A(V[j])
+        h = np.array([np.sum(v * w) for v in V])
+        w = w - sum(hi * v for hi, v in zip(h, V))
+        H[:j + 1, j] = h
+        H[j + 1, j] = np.linalg.norm(w)
+        V.append(w / H[j + 1, j])
+    e = np.zeros(k + 1)
+    e[0] = beta
+    y = np.linalg.lstsq(H, e, rcond=None)[0]
+    return sum(yi * v for yi, v in zip(y, V))
+
+
+@pytest.mark.parametrize("n", [16, 18, 48])
+def test_coarse_sizes_match_oracle(fixture_loader, n):
+    meta, arr = fixture_loader("water_hnc_n24")
+    ctx = RismContext(meta["solute"], meta["solvent"], settings_of(meta, N=n, **{"coarse-h": 0}), arr["chi"])
+    P = problem(meta, arr["chi"], n)
+    rng = np.random.default_rng(11)
+    T = 0.3 * rng.standard_normal(ctx.shape)
+    dT = rng.standard_normal(ctx.shape)
+    F_ref, J_ref = P.iterate_t1(T), P.jacobian_t1(T, dT)
+    for dt, tol in ((torch.float64, 1e-11), (torch.float32, 2e-5)):
+        F = ctx.iterate_t1(to_dev(T, dt))[0].double().cpu().numpy()
+        J = ctx.jacobian_t1(to_dev(T, dt), to_dev(dT, dt)).double().cpu().numpy()
+        assert np.max(np.abs(F - F_ref)) < tol * np.max(np.abs(F_ref)), dt
+        assert np.max(np.abs(J - J_ref)) < tol * np.max(np.abs(J_ref)), dt
+    ctx.close()
+
+
+@pytest.mark.parametrize("name", ["water_hnc_n24", "synth6_kh_n32"])
+def test_preconditioner_matches_numpy(fixture_loader, name):
+    meta, arr = fixture_loader(name)
+    steps = 12
+    ctx = RismContext(meta["solute"], meta["solvent"], settings_of(meta, **{"coarse-steps": steps}), arr["chi"])
+    s = meta["settings"]
+    N = s["N"]
+    nc = ctx.coarse_grid()
+    assert nc is not None and nc[0] < N
+    R, Pm = transfer(N, nc[0])
+    Pc = problem(meta, arr["chi"], nc[0])
+    rng = np.random.default_rng(3)
+    for T in (arr["T"], 0.5 * rng.standard_normal(ctx.shape)):  # converged and far-off states
+        v = rng.standard_normal(ctx.shape)
+        z = ctx.precondition(to_dev(T), to_dev(v)).cpu().numpy()
+        d = cl.closure1(int(s["closure"]), s["beta"], problem(meta, arr["chi"], N).v, T, np.ones_like(T))
+        dH = along(R, d)
+
+        def JH(u):
+            return Pc.ifft(Pc.star(Pc.fft(dH * u) * Pc.h3)) * (1.0 / Pc.L3) - u
+
+        rc = along(R, v)
+        z_ref = along(Pm, gmres_steps(JH, rc, steps) + rc) - v
+        assert np.max(np.abs(z - z_ref)) < 1e-4 * np.max(np.abs(z_ref))
+    ctx.close()
+
+
+@pytest.mark.parametrize("name", ["water_hnc_n24", "synth6_kh_n32", "synth6_pse3_n32"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_preconditioned_solve_reaches_the_root(fixture_loader, name, precision):
+    meta, arr = fixture_loader(name)
+    out = hnc3d_run_solute(meta["solute"], meta["solvent"],
+                           settings_of(meta, **{"norm-tol": 1e-12, "precision": precision}), arr["chi"])
+    assert out["jv-evals-coarse"] > 0
+    assert out["resid-inf"] < 1e-12
+    assert abs(out["free-energy"] - meta["mu"]) < 1e-6
+    assert np.max(np.abs(out["RESTART"] - arr["T"])) < 1e-10
