@@ -68,15 +68,18 @@ __global__ void __launch_bounds__(256) k_mdotv(long long nw, const T *__restrict
 }
 
 // w = ws * w - sum_v c_v V_v; part[b] = block b's sum of w^2 (if part).
+// c_v = cf.c[v], times dcoef[v] when dcoef (device-resident coefficients,
+// e.g. dot products reduced on the device) is given.
 template <typename T>
 __global__ void __launch_bounds__(256) k_maxpyv(long long nw, T *__restrict__ w, double ws, int nv, VecSet<T> vs,
-                                               Coefs cf, double *__restrict__ part) {
+                                               Coefs cf, const double *__restrict__ dcoef,
+                                               double *__restrict__ part) {
   using VT = typename Wide<T>::type;
   constexpr int WN = Wide<T>::n;
   // the update runs in the basis precision; coefficients converted once
   T c[kVecMax];
 #pragma unroll
-  for (int v = 0; v < kVecMax; ++v) c[v] = (T)cf.c[v];
+  for (int v = 0; v < kVecMax; ++v) c[v] = (T)(dcoef ? (v < nv ? cf.c[v] * dcoef[v] : 0.0) : cf.c[v]);
   const T wsT = (T)ws;
   double s2 = 0.0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += (long long)gridDim.x * blockDim.x) {
@@ -134,6 +137,52 @@ __global__ static void __launch_bounds__(kVecMax * 8) k_colsum(int nblk, int str
     for (int q = 0; q < 8; ++q) s += sm[q][v];
     out[v] = s;
   }
+}
+
+// w /= sqrt(*nrm2) (w = 0 when the norm is 0); the norm goes to *hout.
+// Used by the device-driven GMRES, whose basis is normalised explicitly.
+template <typename T>
+__global__ void k_scale_norm(long long n, T *__restrict__ w, const double *__restrict__ nrm2,
+                             double *__restrict__ hout) {
+  const double s = sqrt(fmax(*nrm2, 0.0));
+  if (hout && blockIdx.x == 0 && threadIdx.x == 0) *hout = s;
+  const T inv = s > 0.0 ? (T)(1.0 / s) : T(0);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    w[i] *= inv;
+}
+
+// Least squares of a k-step Arnoldi run, on one thread: min |beta e1 - H y|
+// with H's column j at H[j * (k + 1) + i], i <= j + 1; then y[0] += beta,
+// so that sum y_j V_j = x + r0 (the GMRES iterate plus its right-hand side).
+__global__ static void k_arnoldi_lsq(int k, const double *__restrict__ H, const double *__restrict__ beta,
+                                     double *__restrict__ y) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double R[kVecMax][kVecMax + 1];  // R[i][j], i <= j + 1
+  double g[kVecMax + 1], cs[kVecMax], sn[kVecMax];
+  for (int j = 0; j < k; ++j)
+    for (int i = 0; i <= j + 1; ++i) R[i][j] = H[j * (k + 1) + i];
+  for (int i = 0; i <= k; ++i) g[i] = 0.0;
+  g[0] = *beta;
+  for (int j = 0; j < k; ++j) {
+    for (int i = 0; i < j; ++i) {
+      const double a = R[i][j], b = R[i + 1][j];
+      R[i][j] = cs[i] * a + sn[i] * b;
+      R[i + 1][j] = -sn[i] * a + cs[i] * b;
+    }
+    const double a = R[j][j], b = R[j + 1][j];
+    const double r = hypot(a, b);
+    cs[j] = r == 0.0 ? 1.0 : a / r;
+    sn[j] = r == 0.0 ? 0.0 : b / r;
+    R[j][j] = r;
+    g[j + 1] = -sn[j] * g[j];
+    g[j] = cs[j] * g[j];
+  }
+  for (int i = k - 1; i >= 0; --i) {
+    double s = g[i];
+    for (int l = i + 1; l < k; ++l) s -= R[i][l] * y[l];
+    y[i] = R[i][i] != 0.0 ? s / R[i][i] : 0.0;
+  }
+  if (k > 0) y[0] += *beta;
 }
 
 }  // namespace rism

@@ -178,6 +178,12 @@ struct rism3d_ctx {
   float *tA = nullptr, *tB = nullptr;       // partially transferred fields
   float *tc_r = nullptr, *tc_y = nullptr;   // coarse right-hand side / solution
   int coarse_jv = 0;
+  // the coarse solve as one CUDA graph (device-driven GMRES, no host syncs)
+  cudaGraph_t cg_graph = nullptr;
+  cudaGraphExec_t cg_exec = nullptr;
+  double *cg_H = nullptr, *cg_aux = nullptr;  // Hessenberg columns; norm, beta, y
+  long long cg_nodes = 0;
+  bool cg_failed = false;
 
   cudaStream_t stream = 0;
   PassTimer timer;
@@ -202,7 +208,9 @@ struct rism3d_ctx {
     for (auto p : zbasis64) fr(p);
     for (auto p : zbasis32) fr(p);
     for (int a = 0; a < 3; ++a) { fr(tR[a]); fr(tRt[a]); fr(tP[a]); fr(tPt[a]); }
-    fr(tA); fr(tB); fr(tc_r); fr(tc_y);
+    fr(tA); fr(tB); fr(tc_r); fr(tc_y); fr(cg_H); fr(cg_aux);
+    if (cg_exec) cudaGraphExecDestroy(cg_exec);
+    if (cg_graph) cudaGraphDestroy(cg_graph);
     delete coarse;
     if (timer.on) { cudaEventDestroy(timer.a); cudaEventDestroy(timer.b); }
   }
@@ -529,7 +537,7 @@ double maxpy(rism3d_ctx *c, T *w, double ws, const std::vector<VecRef<T>> &V, co
       cf.c[i] = i < k ? coef[base + i] * V[base + i].s : 0.0;
     }
     const bool last = base + kVecMax >= nv;
-    k_maxpyv<T><<<G, 256, 0, c->stream>>>(nw, w, base == 0 ? ws : 1.0, std::max(k, 0), vs, cf,
+    k_maxpyv<T><<<G, 256, 0, c->stream>>>(nw, w, base == 0 ? ws : 1.0, std::max(k, 0), vs, cf, nullptr,
                                            (last && want_norm) ? c->dpart : nullptr);
     CKL();
   }
@@ -732,19 +740,120 @@ template <typename T> void tg_prepare(rism3d_ctx *c, const T *d) {
   tg_restrict<T>(c, d, 1.0, slopebuf<float>(c->coarse));
 }
 
+int coarse_steps(const rism3d_ctx *c) {
+  return c->pd.coarse_steps > 0 ? std::min(c->pd.coarse_steps, kVecMax - 1) : 12;
+}
+
+// The coarse solve driven entirely on the device: k GMRES steps from zero
+// on J_H with an explicitly normalised basis, the dot products and norms
+// reduced into device memory, the small least-squares problem solved by one
+// thread, and tc_y = sum y_j V_j = J_H^-1 r + r written at the end.  On
+// entry the coarse basis vector 0 holds r; nothing here waits for the host,
+// so the whole sequence is captured once as a CUDA graph.
+void coarse_solve_dev(rism3d_ctx *c, int k) {
+  rism3d_ctx *cc = c->coarse;
+  auto &B = basis<float>(cc);
+  const float *d = cc->d32;
+  const int G = cc->red_blocks;
+  const long long nw = cc->nvec / Wide<float>::n;
+  const int gv = vec_grid(cc->nvec);
+  cudaStream_t st = cc->stream;
+  double *H = c->cg_H, *nrm = c->cg_aux, *beta = c->cg_aux + 1, *y = c->cg_aux + 2;
+  Coefs one{}, mone{};
+  for (int i = 0; i < kVecMax; ++i) one.c[i] = 1.0, mone.c[i] = -1.0;
+  k_maxpyv<float><<<G, 256, 0, st>>>(nw, B[0], 1.0, 0, VecSet<float>{}, one, nullptr, cc->dpart);
+  k_colsum<<<1, kVecMax * 8, 0, st>>>(G, 1, 1, cc->dpart, nrm);  // |r|^2
+  k_scale_norm<float><<<gv, 256, 0, st>>>(cc->nvec, B[0], nrm, beta);
+  CKL();
+  for (int j = 0; j < k; ++j) {
+    pipeline<float, MODE_J>(cc, B[j], d, 1.f, 1.f, B[j + 1]);
+    VecSet<float> vs{};
+    for (int i = 0; i < kVecMax; ++i) vs.p[i] = B[i <= j ? i : 0];
+    double *h = H + (size_t)j * (k + 1);
+    k_mdotv<float><<<G, 256, 0, st>>>(nw, B[j + 1], j + 1, vs, cc->dpart);
+    k_colsum<<<1, kVecMax * 8, 0, st>>>(G, kVecMax, j + 1, cc->dpart, h);
+    k_maxpyv<float><<<G, 256, 0, st>>>(nw, B[j + 1], 1.0, j + 1, vs, one, h, cc->dpart);
+    k_colsum<<<1, kVecMax * 8, 0, st>>>(G, 1, 1, cc->dpart, nrm);
+    k_scale_norm<float><<<gv, 256, 0, st>>>(cc->nvec, B[j + 1], nrm, h + j + 1);
+    CKL();
+  }
+  k_arnoldi_lsq<<<1, 1, 0, st>>>(k, H, beta, y);
+  VecSet<float> vs{};
+  for (int i = 0; i < kVecMax; ++i) vs.p[i] = B[i < k ? i : 0];
+  k_maxpyv<float><<<G, 256, 0, st>>>(nw, c->tc_y, 0.0, k, vs, mone, y, nullptr);
+  CKL();
+}
+
+// Capture coarse_solve_dev once (on a private stream; it is launched into the
+// context's stream afterwards).  False, with the host-driven path left to
+// the caller, when capture or instantiation fails.
+bool coarse_graph(rism3d_ctx *c, int k) {
+  if (c->cg_exec) return true;
+  if (c->cg_failed) return false;
+  const char *env = std::getenv("RISM3D_COARSE_GRAPH");  // 0: host-driven coarse GMRES
+  if (env && env[0] == '0') {
+    c->cg_failed = true;
+    return false;
+  }
+  rism3d_ctx *cc = c->coarse;
+  ensure_basis<float>(cc, k + 1);  // every buffer the graph touches exists before capture
+  slopebuf<float>(cc);
+  if (!c->cg_H) c->cg_H = dalloc<double>((size_t)k * (k + 1));
+  if (!c->cg_aux) c->cg_aux = dalloc<double>((size_t)k + 2);
+  cudaStream_t cap = nullptr;
+  CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  cudaStream_t saved = cc->stream;
+  cc->stream = cap;
+  cudaGraph_t g = nullptr;
+  bool ok = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    try {
+      coarse_solve_dev(c, k);
+    } catch (const CudaFail &) {
+      ok = false;
+    }
+    if (cudaStreamEndCapture(cap, &g) != cudaSuccess) ok = false;
+  }
+  cc->stream = saved;
+  cudaStreamDestroy(cap);
+  if (ok && g) {
+    size_t n = 0;
+    ok = cudaGraphGetNodes(g, nullptr, &n) == cudaSuccess &&
+         cudaGraphInstantiate(&c->cg_exec, g, 0) == cudaSuccess;
+    c->cg_nodes = (long long)n;
+  }
+  if (ok) {
+    c->cg_graph = g;
+  } else {
+    if (g) cudaGraphDestroy(g);
+    c->cg_exec = nullptr;
+    c->cg_failed = true;
+    cudaGetLastError();  // capture errors are not sticky; clear the record
+  }
+  return ok;
+}
+
 // z = M^-1 (s v).
 template <typename T> void tg_apply(rism3d_ctx *c, const T *v, double s, T *z) {
   rism3d_ctx *cc = c->coarse;
   const int prec = sizeof(T) == 8 ? 0 : 1;
+  const int k = coarse_steps(c);
+  const bool graph = coarse_graph(c, k);
   const long long l0 = launch_total(cc);
   {
     TimeScope ts(c, TK_PREC, prec, 6);
-    tg_restrict<T>(c, v, s, c->tc_r);
-    const int k = c->pd.coarse_steps > 0 ? std::min(c->pd.coarse_steps, 100) : 12;
-    const int jv0 = cc->jv32_evals;
-    gmres<float>(cc, slopebuf<float>(cc), c->tc_r, c->tc_y, 0.0, k, k);
-    c->coarse_jv += cc->jv32_evals - jv0;
-    axpby<float, float>(cc, 1.0, c->tc_r, 1.0, c->tc_y);
+    if (graph) {
+      tg_restrict<T>(c, v, s, basis<float>(cc)[0]);
+      CK(cudaGraphLaunch(c->cg_exec, c->stream));
+      c->timer.launches[TK_PREC + 6 * prec] += c->cg_nodes;
+      c->coarse_jv += k;
+    } else {
+      tg_restrict<T>(c, v, s, c->tc_r);
+      const int jv0 = cc->jv32_evals;
+      gmres<float>(cc, slopebuf<float>(cc), c->tc_r, c->tc_y, 0.0, k, k);
+      c->coarse_jv += cc->jv32_evals - jv0;
+      axpby<float, float>(cc, 1.0, c->tc_r, 1.0, c->tc_y);
+    }
     tg_prolong<T>(c, c->tc_y, v, s, z);
   }
   c->timer.launches[TK_PREC + 6 * prec] += launch_total(cc) - l0;
@@ -1081,6 +1190,12 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
       while (t.BZ > 4 && G.N2 * t.BZ > rc * 256) t.BZ /= 2;
       if (G.N1 * t.BY > rc * 256 || G.N2 * t.BZ > rc * 256)
         throw ArgFail{RISM3D_ERR_ARG, "grid too large for the tile shapes"};
+      // small grids (the coarse problem): smaller batches while a pass would
+      // otherwise launch fewer than two CTAs per SM
+      const long long want = 2 * 148;
+      while (t.RX > 4 && (long long)((G.N1 * G.N2 + t.RX - 1) / t.RX) * m < want) t.RX /= 2;
+      while (t.BY > 4 && (long long)((G.Nh + t.BY - 1) / t.BY) * G.N2 * m < want) t.BY /= 2;
+      while (t.BZ > 4 && (long long)((G.Nh + t.BZ - 1) / t.BZ) * G.N1 < want) t.BZ /= 2;
     }
     // |k| of every grid point must fall inside the chi table (interp assert,
     // bgy3d-vec.c:30-31)
@@ -1187,6 +1302,8 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
     CK(cudaDeviceSynchronize());
     cudaFree(d_solvent);
     CK(cudaMalloc(&c->W, sizeof(double2) * (size_t)(m * G.Nc)));
+    // reduction blocks: about four 16-byte loads per thread, at most 4 per SM
+    c->red_blocks = (int)std::min<long long>(592, std::max<long long>(8, (c->nvec / 4 + 1023) / 1024));
     c->dpart = dalloc<double>((size_t)c->red_blocks * kVecMax + 64);
     c->dres = dalloc<double>(4 * kVecMax);
     CK(cudaMallocHost(&c->hres, sizeof(double) * 4 * kVecMax));

@@ -88,8 +88,12 @@ def test_coarse_sizes_match_oracle(fixture_loader, n):
     ctx.close()
 
 
+@pytest.mark.parametrize("graph", ["1", "0"])
 @pytest.mark.parametrize("name", ["water_hnc_n24", "synth6_kh_n32"])
-def test_preconditioner_matches_numpy(fixture_loader, name):
+def test_preconditioner_matches_numpy(fixture_loader, name, graph, monkeypatch):
+    """Both coarse-solve drivers: the device-driven one replayed as a CUDA
+    graph (default) and the host-driven GMRES (RISM3D_COARSE_GRAPH=0)."""
+    monkeypatch.setenv("RISM3D_COARSE_GRAPH", graph)
     meta, arr = fixture_loader(name)
     steps = 12
     ctx = RismContext(meta["solute"], meta["solvent"], settings_of(meta, **{"coarse-steps": steps}), arr["chi"])
