@@ -7,4 +7,5 @@ access to the residual and Jacobian (``RismContext``).
 """
 from ._abi import CLOSURES, RismError, lib  # noqa: F401
 from .sites import MOLECULES, find_molecule, synthetic_solute  # noqa: F401
-from .solver import DEFAULTS, RismContext, hnc3d_run_solute, problem_data, rism_solvent  # noqa: F401
+from .solver import (DEFAULTS, RismContext, hnc3d_run_batch, hnc3d_run_solute, problem_data,  # noqa: F401
+                     rism_solvent)

@@ -52,7 +52,13 @@ class Result(ctypes.Structure):
                 ("newton_iters", ctypes.c_int), ("f_evals", ctypes.c_int),
                 ("jv_evals", ctypes.c_int), ("f_evals_fp32", ctypes.c_int),
                 ("jv_evals_fp32", ctypes.c_int), ("jv_evals_coarse", ctypes.c_int),
-                ("seconds", ctypes.c_double)]
+                ("seconds", ctypes.c_double), ("launches", ctypes.c_longlong)]
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("pd", Problem), ("n", ctypes.c_int), ("solute", ctypes.POINTER(Site)),
+                ("chi", ctypes.POINTER(ctypes.c_double)), ("t_inout", ctypes.POINTER(ctypes.c_double)),
+                ("g_out", ctypes.POINTER(ctypes.c_double)), ("result", Result)]
 
 
 # Every entry point declared in include/rism3d.h (checked by the CPU tests).
@@ -62,7 +68,7 @@ EXPORTS = [
     "rism3d_jacobian_t1", "rism3d_iterate_t1_f32", "rism3d_jacobian_t1_f32",
     "rism3d_solve", "rism3d_observables", "rism3d_get_field", "rism3d_last_error",
     "rism3d_profile", "rism1d_solvent_chi", "rism3d_jacobian_apply_noalloc",
-    "rism3d_precondition", "rism3d_coarse_grid",
+    "rism3d_precondition", "rism3d_coarse_grid", "rism3d_solve_batch",
 ]
 
 _lib = None
@@ -111,6 +117,8 @@ def lib():
     L.rism3d_precondition.restype = I
     L.rism3d_coarse_grid.argtypes = [V, P(I)]
     L.rism3d_coarse_grid.restype = I
+    L.rism3d_solve_batch.argtypes = [I, P(Site), I, P(Job), I]
+    L.rism3d_solve_batch.restype = I
     _lib = L
     return L
 

@@ -31,7 +31,9 @@ def _stale():
 def build(force=False, verbose_ptxas=False):
     if not force and not _stale() and not verbose_ptxas:
         return LIB
-    cmd = [NVCC, "-O3", "-std=c++17", "-lineinfo",
+    # per-thread default streams: host threads of the batch driver issue
+    # independently; each still orders against torch's legacy stream
+    cmd = [NVCC, "-O3", "-std=c++17", "-lineinfo", "--default-stream", "per-thread",
            "-gencode", "arch=compute_100a,code=sm_100a",
            "-Xcompiler", "-fPIC,-O3", "-shared",
            "-I", os.path.join(ROOT, "include"), "-I", CSRC,

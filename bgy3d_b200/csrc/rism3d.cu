@@ -10,12 +10,17 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
+#include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kernels.cuh"
@@ -57,11 +62,53 @@ struct ArgFail {
   std::string msg;
 };
 
+// Device memory comes from the device's stream-ordered pool on the calling
+// thread's default stream (the library is built with per-thread default
+// streams): unlike cudaMalloc / cudaFree it never synchronises the device,
+// so solves set up and torn down by concurrent host threads (the batch
+// driver) do not stall one another.  The pool keeps freed memory for reuse.
+void pool_setup() {
+  static std::mutex mu;
+  static bool done[64] = {false};
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev < 0 || dev >= 64 || done[dev]) return;
+  cudaMemPool_t pool;
+  CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+  uint64_t keep = UINT64_MAX;
+  CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  done[dev] = true;
+}
+
 template <typename T> T *dalloc(size_t count) {
+  pool_setup();
   void *p = nullptr;
   if (count == 0) count = 1;
-  CK(cudaMalloc(&p, count * sizeof(T)));
+  CK(cudaMallocAsync(&p, count * sizeof(T), cudaStreamPerThread));
   return static_cast<T *>(p);
+}
+
+// Stream-ordered free on the calling thread's stream: callers free only
+// memory whose last use was on that stream or has completed.
+void dfree(void *p) {
+  if (p) cudaFreeAsync(p, cudaStreamPerThread);
+}
+
+// Pinned landing buffer of the calling host thread for reduced Krylov
+// coefficients (4 * 32 doubles), allocated on first use and kept for the
+// thread's lifetime: contexts come and go without pinning or unpinning
+// host memory, which would synchronise the device.
+double *pinned_scratch() {
+  struct Buf {
+    double *p = nullptr;
+    ~Buf() {
+      if (p) cudaFreeHost(p);
+    }
+  };
+  static thread_local Buf b;
+  if (!b.p) CK(cudaMallocHost(&b.p, sizeof(double) * 4 * kVecMax));
+  return b.p;
 }
 
 bool is_2a3b(int n) {
@@ -153,7 +200,6 @@ struct rism3d_ctx {
   std::vector<NormPartial> h_npart;
   double *dpart = nullptr;       // [red_blocks][kVecMax] reduction partials
   double *dres = nullptr;        // [kVecMax * 2] reduced coefficients (device)
-  double *hres = nullptr;        // pinned host copy of dres
   std::vector<double> h_dpart;
   int red_blocks = 592;
 
@@ -196,12 +242,11 @@ struct rism3d_ctx {
   int *d_err = nullptr;  // set by a kernel whose bounded wait timed out
 
   ~rism3d_ctx() {
-    auto fr = [](void *p) { if (p) cudaFree(p); };
+    auto fr = [](void *p) { dfree(p); };
     for (int i = 0; i < 3; ++i) { fr(tw64[i]); fr(tw32[i]); }
     fr(post64); fr(post32); fr(v64); fr(v32); fr(L64); fr(L32);
     fr(chi64); fr(s64); fr(chi32); fr(s32); fr(W); fr(d_solute); fr(d_charge);
     fr(npart); fr(dpart); fr(dres); fr(F64); fr(X64t); fr(F64t); fr(X32); fr(F32); fr(X32t); fr(F32t);
-    if (hres) cudaFreeHost(hres);
     fr(d64); fr(d32); fr(dx64); fr(dx32); fr(d_err);
     for (auto p : basis64) fr(p);
     for (auto p : basis32) fr(p);
@@ -311,16 +356,18 @@ bool static_len_x(int M) { return M == 48 || M == 64 || M == 128; }
 bool static_len_yz(int N) { return N == 96 || N == 128 || N == 256; }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  if (!fn) {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {  // thread-safe one-time lookup
     void *p = nullptr;
     cudaDriverEntryPointQueryResult q{};
-    CK(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q));
-    if (q != cudaDriverEntryPointSuccess || !p) {
-      g_last_error = "cuTensorMapEncodeTiled unavailable";
-      throw CudaFail{RISM3D_ERR_CUDA};
-    }
-    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  if (!fn) {
+    g_last_error = "cuTensorMapEncodeTiled unavailable";
+    throw CudaFail{RISM3D_ERR_CUDA};
   }
   return fn;
 }
@@ -514,9 +561,10 @@ void mdot(rism3d_ctx *c, const T *w, double ws, const std::vector<VecRef<T>> &V,
     k_colsum<<<1, kVecMax * 8, 0, c->stream>>>(G, kVecMax, k, c->dpart, c->dres + base);
     CKL();
   }
-  CK(cudaMemcpyAsync(c->hres, c->dres, sizeof(double) * nv, cudaMemcpyDeviceToHost, c->stream));
+  double *hres = pinned_scratch();
+  CK(cudaMemcpyAsync(hres, c->dres, sizeof(double) * nv, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  for (int i = 0; i < nv; ++i) h[i] = c->hres[i] * ws * V[i].s;
+  for (int i = 0; i < nv; ++i) h[i] = hres[i] * ws * V[i].s;
 }
 
 // w = ws * w - sum_i coef_i (s_i V_i); returns ||w||_2 if want_norm.
@@ -544,9 +592,10 @@ double maxpy(rism3d_ctx *c, T *w, double ws, const std::vector<VecRef<T>> &V, co
   if (!want_norm) return 0.0;
   k_colsum<<<1, kVecMax * 8, 0, c->stream>>>(G, 1, 1, c->dpart, c->dres);
   CKL();
-  CK(cudaMemcpyAsync(c->hres, c->dres, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  double *hres = pinned_scratch();
+  CK(cudaMemcpyAsync(hres, c->dres, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  return std::sqrt(c->hres[0]);
+  return std::sqrt(hres[0]);
 }
 
 template <typename TX, typename TY> void axpby(rism3d_ctx *c, double a, const TX *x, double b, TY *y) {
@@ -1040,6 +1089,7 @@ int solve_impl(rism3d_ctx *c, double *T, rism3d_result *out) {
   rism3d_result res{};
   c->f_evals = c->jv_evals = c->f32_evals = c->jv32_evals = 0;
   c->coarse_jv = 0;
+  const long long launches0 = launch_total(c);
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -1101,6 +1151,7 @@ int solve_impl(rism3d_ctx *c, double *T, rism3d_result *out) {
   res.f_evals_fp32 = c->f32_evals;
   res.jv_evals_fp32 = c->jv32_evals;
   res.jv_evals_coarse = c->coarse_jv;
+  res.launches = launch_total(c) - launches0;
   res.seconds = ms * 1e-3;
   if (out) {
     const double keep[5] = {out->mu, out->mu_hnc, out->mu_kh, out->mu_gf, out->pmv_factor};
@@ -1121,12 +1172,13 @@ int observables_impl(rism3d_ctx *c, const double *T, double *g, rism3d_result *o
   CKL();
   ObsPartial *part = dalloc<ObsPartial>(nb);
   k_observables<<<nb, 256, 0, c->stream>>>(G, T, c->v64, uc, pd.beta, pd.closure, c->d_charge, g, part);
+  c->timer.launches[TK_VEC] += 2;
   CKL();
   std::vector<ObsPartial> hp(nb);
   CK(cudaMemcpyAsync(hp.data(), part, sizeof(ObsPartial) * nb, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  cudaFree(part);
-  cudaFree(uc);
+  dfree(part);
+  dfree(uc);
   double s[5] = {0, 0, 0, 0, 0};
   for (unsigned b = 0; b < nb; ++b) {
     s[0] += hp[b].mu; s[1] += hp[b].hnc; s[2] += hp[b].kh; s[3] += hp[b].gf; s[4] += hp[b].csum;
@@ -1299,14 +1351,13 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
     k_longrange<<<(unsigned)((nk + 255) / 256), 256>>>(G, n, c->d_solute, pd->renorm, 1.0 / c->h3, c->L64,
                                                        c->L32);
     CKL();
-    CK(cudaDeviceSynchronize());
-    cudaFree(d_solvent);
-    CK(cudaMalloc(&c->W, sizeof(double2) * (size_t)(m * G.Nc)));
+    CK(cudaStreamSynchronize(cudaStreamPerThread));
+    dfree(d_solvent);
+    c->W = dalloc<double2>((size_t)m * G.Nc);
     // reduction blocks: about four 16-byte loads per thread, at most 4 per SM
     c->red_blocks = (int)std::min<long long>(592, std::max<long long>(8, (c->nvec / 4 + 1023) / 1024));
     c->dpart = dalloc<double>((size_t)c->red_blocks * kVecMax + 64);
     c->dres = dalloc<double>(4 * kVecMax);
-    CK(cudaMallocHost(&c->hres, sizeof(double) * 4 * kVecMax));
     const int rows = G.N1 * G.N2;
     const int rxmin = std::min(std::min(c->tiles[0].RX, c->tiles[1].RX), kStaticRX);
     c->npart = dalloc<NormPartial>((size_t)((rows + rxmin - 1) / rxmin) * m);
@@ -1412,12 +1463,19 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
           const int nf = pd->N[a], ncs = nc[a];
           c->Nc[a] = ncs;
           std::vector<float> R((size_t)ncs * nf), Rt((size_t)nf * ncs), P((size_t)nf * ncs), Pt((size_t)ncs * nf);
+          // s(x) = sum_{|k| <= K} w_k cos(2 pi k x), K = ncs / 2, w_{+-K} = 1/2:
+          // the Dirichlet kernel sin((2K - 1) pi x) / sin(pi x) of |k| < K
+          // plus cos(2 pi K x); x = i/ncs - j/nf = (i nf - j ncs) / (ncs nf)
+          const int K = ncs / 2;
+          const long long den = (long long)ncs * nf;
           for (int i = 0; i < ncs; ++i)
             for (int j = 0; j < nf; ++j) {
-              const double x = (double)i / ncs - (double)j / nf;
-              double s = 0.0;
-              for (int k = -ncs / 2; k <= ncs / 2; ++k)
-                s += (2 * std::abs(k) == ncs ? 0.5 : 1.0) * std::cos(2.0 * pi * k * x);
+              long long q = ((long long)i * nf - (long long)j * ncs) % den;
+              if (q < 0) q += den;
+              const double x = (double)q / (double)den;  // in [0, 1)
+              const double sx = std::sin(pi * x);
+              double s = std::fabs(sx) < 1e-12 ? (double)(2 * K - 1) : std::sin((2 * K - 1) * pi * x) / sx;
+              s += std::cos(2.0 * pi * K * x);
               R[(size_t)i * nf + j] = Rt[(size_t)j * ncs + i] = (float)(s / nf);
               P[(size_t)j * ncs + i] = Pt[(size_t)i * nf + j] = (float)(s / ncs);
             }
@@ -1586,12 +1644,13 @@ int rism3d_solute_solve(const rism3d_problem *pd, int m, const rism3d_site *solv
     const size_t bytes = sizeof(double) * ctx->nvec;
     double *T = dalloc<double>(ctx->nvec);
     double *g = g_out ? dalloc<double>(ctx->nvec) : nullptr;
-    struct Free { double *a, *b; ~Free() { if (a) cudaFree(a); if (b) cudaFree(b); } } fr{T, g};
+    struct Free { double *a, *b; ~Free() { dfree(a); dfree(b); } } fr{T, g};
     if (t_inout) CK(cudaMemcpy(T, t_inout, bytes, cudaMemcpyHostToDevice));
     else CK(cudaMemset(T, 0, bytes));
     rism3d_result r{};
     int st = solve_impl(ctx, T, &r);
     observables_impl(ctx, T, g, &r);
+    r.launches += 2;  // the observables' kernels
     r.status = st;
     if (t_inout) CK(cudaMemcpy(t_inout, T, bytes, cudaMemcpyDeviceToHost));
     if (g_out) CK(cudaMemcpy(g_out, g, bytes, cudaMemcpyDeviceToHost));
@@ -1600,6 +1659,41 @@ int rism3d_solute_solve(const rism3d_problem *pd, int m, const rism3d_site *solv
   });
   rism3d_ctx_destroy(ctx);
   if (out && rc < 0 && out->status == 0) out->status = rc;
+  return rc;
+}
+
+int rism3d_solve_batch(int m, const rism3d_site *solvent, int njobs, rism3d_job *jobs, int workers) {
+  if (njobs < 0 || (njobs > 0 && !jobs) || !solvent || m < 1) return RISM3D_ERR_ARG;
+  if (njobs == 0) return RISM3D_OK;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return RISM3D_ERR_CUDA;
+  const int nw = std::max(1, std::min(workers > 0 ? workers : 8, njobs));
+  // largest grids first, so that the last jobs to start are short ones
+  std::vector<int> order(njobs);
+  std::iota(order.begin(), order.end(), 0);
+  auto cost = [&](int i) {
+    const rism3d_problem &p = jobs[i].pd;
+    return (double)p.N[0] * p.N[1] * p.N[2];
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+  std::atomic<int> next{0};
+  auto work = [&] {
+    // each worker issues on its own per-thread default stream
+    if (cudaSetDevice(dev) != cudaSuccess) return;
+    for (;;) {
+      const int i = next.fetch_add(1);
+      if (i >= njobs) break;
+      rism3d_job &j = jobs[order[i]];
+      rism3d_solute_solve(&j.pd, m, solvent, j.n, j.solute, j.chi, j.t_inout, j.g_out, &j.result);
+    }
+    cudaStreamSynchronize(cudaStreamPerThread);
+  };
+  std::vector<std::thread> pool;
+  pool.reserve(nw);
+  for (int w = 0; w < nw; ++w) pool.emplace_back(work);
+  for (auto &t : pool) t.join();
+  int rc = RISM3D_OK;
+  for (int i = 0; i < njobs && rc == RISM3D_OK; ++i) rc = jobs[i].result.status;
   return rc;
 }
 

@@ -90,7 +90,7 @@ def _result_dict(r):
         "status": r.status, "newton-iters": r.newton_iters, "f-evals": r.f_evals,
         "jv-evals": r.jv_evals, "f-evals-fp32": r.f_evals_fp32, "jv-evals-fp32": r.jv_evals_fp32,
         "jv-evals-coarse": r.jv_evals_coarse,
-        "seconds": r.seconds,
+        "seconds": r.seconds, "launches": r.launches,
     }
 
 
@@ -149,6 +149,54 @@ def hnc3d_run_solute(solute, solvent, settings, chi, restart=None, want_g=True, 
     out["GUV"] = g
     out["RESTART"] = t
     return out
+
+
+def hnc3d_run_batch(solutes, solvent, settings, chi, workers=0, want_g=False, restarts=None):
+    """Many solute solves in one solvent (rism3d_solve_batch), concurrently.
+
+    solutes: list of site lists.  settings / chi: one for all, or one per
+    solute (each chi [m][m][nrad] matching its settings' rmax / nrad).
+    restarts: None or a list of initial t (or None) per solute.  Returns one
+    result dict per solute, as hnc3d_run_solute (GUV only with want_g,
+    RESTART only where a restart was given); a job that did not converge
+    has its status code in "status" and does not raise.
+    """
+    L = _abi.lib()
+    nj = len(solutes)
+    per = lambda x: x if isinstance(x, (list, tuple)) else [x] * nj  # noqa: E731
+    sets, chis, rests = per(settings), per(chi), per(restarts) if restarts is not None else [None] * nj
+    m = len(solvent)
+    jobs = (_abi.Job * max(1, nj))()
+    keep = []
+    outs = []
+    for i, solute in enumerate(solutes):
+        pd = problem_data(sets[i])
+        c = np.ascontiguousarray(chis[i], dtype=np.float64)
+        if c.shape != (m, m, pd.nrad):
+            raise ValueError(f"chi {i} must be [{m}][{m}][{pd.nrad}], got {c.shape}")
+        shape = (m, pd.N[2], pd.N[1], pd.N[0])
+        t = None if rests[i] is None else np.array(rests[i], dtype=np.float64, order="C", copy=True)
+        if t is not None and t.shape != shape:
+            raise ValueError(f"restart {i} has the wrong shape")
+        g = np.empty(shape) if want_g else None
+        sites = _sites(solute)
+        keep += [c, t, g, sites]
+        jobs[i].pd = pd
+        jobs[i].n = len(solute)
+        jobs[i].solute = ctypes.cast(sites, ctypes.POINTER(_abi.Site))
+        jobs[i].chi = _dptr(c)
+        jobs[i].t_inout = _dptr(t) if t is not None else None
+        jobs[i].g_out = _dptr(g) if g is not None else None
+        outs.append((t, g))
+    rc = L.rism3d_solve_batch(m, _sites(solvent), nj, jobs, int(workers))
+    if rc in (_abi.ERR_ARG, _abi.ERR_CUDA) and all(jobs[i].result.status == 0 for i in range(nj)):
+        raise _abi.RismError(rc, "hnc3d_run_batch")
+    results = []
+    for i in range(nj):
+        d = _result_dict(jobs[i].result)
+        d["RESTART"], d["GUV"] = outs[i]
+        results.append(d)
+    return results
 
 
 class RismContext:

@@ -113,6 +113,8 @@ typedef struct rism3d_result {
   int f_evals_fp32, jv_evals_fp32;
   int jv_evals_coarse; /* J.v products on the coarse grid (preconditioner) */
   double seconds;     /* device time of the non-linear solve */
+  long long launches; /* kernels this library launched for the solve (a
+                         replayed CUDA graph counts its kernel nodes) */
 } rism3d_result;
 
 /* Defaults of bgy3d-guile.c:243-386 / guile/bgy3d.scm:323-340 for a cubic
@@ -138,6 +140,32 @@ int rism3d_solute_solve(const rism3d_problem *pd,
                         const double *chi,
                         double *t_inout, double *g_out,
                         rism3d_result *out);
+
+/* One solute of a batch: the arguments of rism3d_solute_solve for that
+   solute (its own problem -- grid, box, closure, precision -- and chi
+   table) and its result. */
+typedef struct rism3d_job {
+  rism3d_problem pd;
+  int n;                      /* solute sites */
+  const rism3d_site *solute;  /* host, borrowed */
+  const double *chi;          /* [m][m][pd.nrad] host, borrowed (may be shared) */
+  double *t_inout;            /* host [m][N2][N1][N0] or NULL, as above */
+  double *g_out;              /* host [m][N2][N1][N0] or NULL */
+  rism3d_result result;       /* out; result.status is the job's code */
+} rism3d_job;
+
+/*
+  Many independent solute solves in one solvent, of uneven site counts and
+  grid sizes (a set of solutes or the points of a PES scan: the loops over
+  hnc3d_solute_solve calls in guile/bgy3d.scm:819-880, 943-975), solved
+  concurrently on the current device: `workers` host threads (0: 8), each
+  issuing on its own CUDA stream, take the jobs largest grid first; device
+  memory comes from the stream-ordered pool, so no job's setup or teardown
+  synchronises the device.  Returns RISM3D_OK when every job converged,
+  otherwise the code of the first failing job in job order (every job still
+  runs; see jobs[i].result.status).
+*/
+int rism3d_solve_batch(int m, const rism3d_site *solvent, int njobs, rism3d_job *jobs, int workers);
 
 /* ---- device-resident context: the inner plug points ------------------ */
 

@@ -40,9 +40,11 @@ def test_struct_layout_matches_header(lib):
     #include <stddef.h>
     #include "rism3d.h"
     int main(void) {
-      printf("%zu %zu %zu %zu %zu %zu\n", sizeof(rism3d_site), sizeof(rism3d_problem),
+      printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(rism3d_site), sizeof(rism3d_problem),
              sizeof(rism3d_result), offsetof(rism3d_problem, precision),
-             offsetof(rism3d_result, seconds), offsetof(rism3d_site, charge));
+             offsetof(rism3d_result, seconds), offsetof(rism3d_site, charge),
+             offsetof(rism3d_problem, coarse_h), offsetof(rism3d_problem, coarse_steps),
+             sizeof(rism3d_job), offsetof(rism3d_job, chi), offsetof(rism3d_job, result));
       return 0;
     }
     """
@@ -53,7 +55,9 @@ def test_struct_layout_matches_header(lib):
         subprocess.run(["gcc", "-I", os.path.dirname(HEADER), c, "-o", exe], check=True)
         got = [int(x) for x in subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()]
     want = [ctypes.sizeof(_abi.Site), ctypes.sizeof(_abi.Problem), ctypes.sizeof(_abi.Result),
-            _abi.Problem.precision.offset, _abi.Result.seconds.offset, _abi.Site.charge.offset]
+            _abi.Problem.precision.offset, _abi.Result.seconds.offset, _abi.Site.charge.offset,
+            _abi.Problem.coarse_h.offset, _abi.Problem.coarse_steps.offset,
+            ctypes.sizeof(_abi.Job), _abi.Job.chi.offset, _abi.Job.result.offset]
     assert got == want
 
 
