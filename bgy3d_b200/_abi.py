@@ -61,6 +61,12 @@ class Job(ctypes.Structure):
                 ("g_out", ctypes.POINTER(ctypes.c_double)), ("result", Result)]
 
 
+class Grad(ctypes.Structure):
+    _fields_ = [("dq", ctypes.POINTER(ctypes.c_double)), ("dsigma", ctypes.POINTER(ctypes.c_double)),
+                ("depsilon", ctypes.POINTER(ctypes.c_double)), ("dx", ctypes.POINTER(ctypes.c_double)),
+                ("adjoint_jv", ctypes.c_int), ("adjoint_resid", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+
 # Every entry point declared in include/rism3d.h (checked by the CPU tests).
 EXPORTS = [
     "rism3d_problem_defaults", "rism3d_solute_solve", "rism3d_ctx_create",
@@ -69,6 +75,7 @@ EXPORTS = [
     "rism3d_solve", "rism3d_observables", "rism3d_get_field", "rism3d_last_error",
     "rism3d_profile", "rism1d_solvent_chi", "rism3d_jacobian_apply_noalloc",
     "rism3d_precondition", "rism3d_coarse_grid", "rism3d_solve_batch",
+    "rism3d_solute_grad", "rism3d_gradient", "rism3d_jacobian_transpose_t1",
 ]
 
 _lib = None
@@ -119,6 +126,12 @@ def lib():
     L.rism3d_coarse_grid.restype = I
     L.rism3d_solve_batch.argtypes = [I, P(Site), I, P(Job), I]
     L.rism3d_solve_batch.restype = I
+    L.rism3d_solute_grad.argtypes = [P(Problem), I, P(Site), I, P(Site), P(D), P(D), P(Result), P(Grad)]
+    L.rism3d_solute_grad.restype = I
+    L.rism3d_gradient.argtypes = [V, V, P(Grad)]
+    L.rism3d_gradient.restype = I
+    L.rism3d_jacobian_transpose_t1.argtypes = [V, V, V, V]
+    L.rism3d_jacobian_transpose_t1.restype = I
     _lib = L
     return L
 

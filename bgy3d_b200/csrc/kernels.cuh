@@ -29,7 +29,9 @@ constexpr int kMaxSites = 6;          // solvent sites m
 constexpr double kEps0Inv = 331.84164;  // EPSILON0INV, bgy3d.h:145
 constexpr double kG = 1.2;              // G_COULOMB_INVERSE_RANGE, bgy3d-solvents.h:9
 
-enum { MODE_F = 0, MODE_J = 1 };
+// MODE_FWD: plain forward 3D transform of A (x and z passes; the z pass
+// stops after its forward transform), used by the gradient.
+enum { MODE_F = 0, MODE_J = 1, MODE_FWD = 2 };
 enum { CL_HNC = 0, CL_KH = 1, CL_PY = 2, CL_PSE0 = 3 };
 
 struct Geo {
@@ -165,6 +167,9 @@ __global__ void __launch_bounds__(256) k_xfwd(Geo g, AxisPlan px, int RX, const 
       if (MODE == MODE_F) {
         z.x = closure_c<T>(closure, p * b.x, a.x);
         z.y = closure_c<T>(closure, p * b.y, a.y);
+      } else if (MODE == MODE_FWD) {
+        z.x = a.x * p;
+        z.y = a.y * p;
       } else {
         z.x = b.x * (a.x * p);
         z.y = b.y * (a.y * p);
@@ -267,6 +272,15 @@ __global__ void __launch_bounds__(256) k_z(Geo g, AxisPlan pz, typename Cx<T>::t
   }
   __syncthreads();
   for (int s = 0; s < m; ++s) fft_tile<false, true>(buf + s * B, pz, B, mB, 1, tw);
+  if (MODE == MODE_FWD) {
+    __syncthreads();
+    for (int e = tid; e < N2 * mB; e += nthr) {
+      const int z = e / mB, r = e - z * mB;
+      const int s = r / B, b = r - s * B;
+      if (b < bw) W[(long long)s * g.Nc + z * zstride + col + b] = buf[e];
+    }
+    return;
+  }
   const int ky = kfreq(y, g.N1);
   const double k1 = ky * g.dk1;
   for (int e = tid; e < N2 * B; e += nthr) {

@@ -25,6 +25,7 @@
 
 #include "kernels.cuh"
 #include "kernels_static.cuh"
+#include "grad.cuh"
 #include "krylov.cuh"
 #include "rism3d.h"
 #include "twogrid.cuh"
@@ -193,7 +194,7 @@ struct rism3d_ctx {
   double2 *chi64 = nullptr, *s64 = nullptr;
   float2 *chi32 = nullptr, *s32 = nullptr;
   void *W = nullptr;  // complex work buffer, FP64-sized, reused by the FP32 path
-  SiteP *d_solute = nullptr;
+  SiteP *d_solute = nullptr, *d_solvent = nullptr;
   double *d_charge = nullptr;
 
   NormPartial *npart = nullptr;
@@ -245,7 +246,7 @@ struct rism3d_ctx {
     auto fr = [](void *p) { dfree(p); };
     for (int i = 0; i < 3; ++i) { fr(tw64[i]); fr(tw32[i]); }
     fr(post64); fr(post32); fr(v64); fr(v32); fr(L64); fr(L32);
-    fr(chi64); fr(s64); fr(chi32); fr(s32); fr(W); fr(d_solute); fr(d_charge);
+    fr(chi64); fr(s64); fr(chi32); fr(s32); fr(W); fr(d_solute); fr(d_solvent); fr(d_charge);
     fr(npart); fr(dpart); fr(dres); fr(F64); fr(X64t); fr(F64t); fr(X32); fr(F32); fr(X32t); fr(F32t);
     fr(d64); fr(d32); fr(dx64); fr(dx32); fr(d_err);
     for (auto p : basis64) fr(p);
@@ -1195,6 +1196,163 @@ int observables_impl(rism3d_ctx *c, const double *T, double *g, rism3d_result *o
   return RISM3D_OK;
 }
 
+// ------------------------------------------------------------- gradient
+// Plain forward 3D transform of an FP64 field into W (runtime-length passes).
+void fwd3d(rism3d_ctx *c, const double *A) {
+  const Geo &G = c->g;
+  auto *W = c->work<double>();
+  const TileShape &t = c->tl<double>();
+  dim3 gx((G.N1 * G.N2 + t.RX - 1) / t.RX, c->m);
+  k_xfwd<double, MODE_FWD><<<gx, 256, xsmem<double>(c), c->stream>>>(G, c->plan<double>(0), t.RX, A, A, 1.0,
+                                                                     c->pd.closure, W, postw<double>(c));
+  CKL();
+  dim3 gy((G.Nh + t.BY - 1) / t.BY, G.N2, c->m);
+  const size_t sy = ysmem<double>(c);
+  if (t.BY == 16) k_y<double, false, 16><<<gy, 256, sy, c->stream>>>(G, c->plan<double>(1), W);
+  else if (t.BY == 8) k_y<double, false, 8><<<gy, 256, sy, c->stream>>>(G, c->plan<double>(1), W);
+  else k_y<double, false, 4><<<gy, 256, sy, c->stream>>>(G, c->plan<double>(1), W);
+  CKL();
+  dim3 gz((G.Nh + t.BZ - 1) / t.BZ, G.N1);
+  const size_t sz = zsmem<double>(c);
+  const ZParams<double> zp = zparams<double>(c, false);
+  if (t.BZ == 16) k_z<double, MODE_FWD, 16><<<gz, 256, sz, c->stream>>>(G, c->plan<double>(2), W, zp);
+  else if (t.BZ == 8) k_z<double, MODE_FWD, 8><<<gz, 256, sz, c->stream>>>(G, c->plan<double>(2), W, zp);
+  else k_z<double, MODE_FWD, 4><<<gz, 256, sz, c->stream>>>(G, c->plan<double>(2), W, zp);
+  CKL();
+  c->timer.launches[TK_XFWD] += 3;
+}
+
+// out = K v = (chi - 1) * v (the OZ convolution alone): the J.v passes with
+// unit slope and nothing subtracted.
+void kconv(rism3d_ctx *c, const double *ones, const double *v, double *out) {
+  pipeline<double, MODE_J>(c, v, ones, 1.0, 0.0, out);
+}
+
+double *ones_field(rism3d_ctx *c) {
+  double *o = dalloc<double>(c->nvec);
+  k_fill<<<vec_grid(c->nvec), 256, 0, c->stream>>>(c->nvec, 1.0, o);
+  CKL();
+  return o;
+}
+
+int jacobian_transpose_impl(rism3d_ctx *c, const double *T, const double *dT, double *out) {
+  double *d = slopebuf<double>(c);
+  closure_slope<double, double>(c, T, d);
+  double *ones = ones_field(c);
+  double *kv = dalloc<double>(c->nvec);
+  kconv(c, ones, dT, kv);
+  k_dmul_sub<<<vec_grid(c->nvec), 256, 0, c->stream>>>(c->nvec, d, kv, dT, out);
+  CKL();
+  CK(cudaStreamSynchronize(c->stream));
+  dfree(kv);
+  dfree(ones);
+  return RISM3D_OK;
+}
+
+// dmu/d(q, sigma, eps, x) of every solute site at the converged T.  The
+// adjoint J^T lambda = b (b = dmu/dt) is solved through the forward
+// Jacobian: with J = K D - 1 and J^T = D K - 1, lambda = D y - b where
+// J y = K b, so the preconditioned FGMRES of the Newton steps serves.
+int gradient_impl(rism3d_ctx *c, const double *T, rism3d_grad *gr) {
+  const rism3d_problem &pd = c->pd;
+  if (!pd.renorm) {
+    g_last_error = "the gradient is implemented for the renormalised form only";
+    return RISM3D_ERR_UNSUPPORTED;
+  }
+  const Geo &G = c->g;
+  const long long nv = c->nvec;
+  const double h0 = pd.L[0] / pd.N[0], h1 = pd.L[1] / pd.N[1], h2 = pd.L[2] / pd.N[2];
+  const double rhoh3 = pd.rho * c->h3, rhoh3b = rhoh3 / pd.beta;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, c->stream));
+  const unsigned nb = (unsigned)((G.Nr + 255) / 256);
+  double *uc = dalloc<double>(G.Nr);
+  k_coulomb_long<<<nb, 256, 0, c->stream>>>(G, h0, h1, h2, pd.L[0], pd.L[1], pd.L[2], c->n, c->d_solute, uc);
+  CKL();
+  double *d = slopebuf<double>(c);
+  closure_slope<double, double>(c, T, d);
+  double *ones = ones_field(c);
+  double *b = dalloc<double>(nv), *y = dalloc<double>(nv), *w = dalloc<double>(nv), *Bw = dalloc<double>(G.Nr);
+  k_mu_dt<<<nb, 256, 0, c->stream>>>(G, T, c->v64, uc, pd.beta, pd.closure, c->d_charge, rhoh3b, b);
+  CKL();
+  const double bnorm = maxpy<double>(c, b, 1.0, {}, {}, true);
+  // J y = K b; lambda = d y - b (into w)
+  kconv(c, ones, b, w);
+  const int restart = pd.krylov_restart > 0 ? std::min(pd.krylov_restart, 200) : 30;
+  const int jv0 = c->jv_evals;
+  if (c->coarse) {
+    tg_prepare<double>(c, d);
+    fgmres<double>(c, d, w, y, 1e-11, 4000, restart);
+  } else {
+    gmres<double>(c, d, w, y, 1e-11, 4000, restart);
+  }
+  gr->adjoint_jv = c->jv_evals - jv0;
+  k_dmul_sub<<<vec_grid(nv), 256, 0, c->stream>>>(nv, d, y, b, w);
+  CKL();
+  double *lam = w;
+  // K lambda (into y); adjoint residual d K lambda - lambda - b (into b)
+  kconv(c, ones, lam, y);
+  k_dmul_sub<<<vec_grid(nv), 256, 0, c->stream>>>(nv, d, y, lam, ones);  // ones <- J^T lambda
+  CKL();
+  xpay<double, double, double>(c, ones, -1.0, b, b);  // b <- J^T lambda - b
+  gr->adjoint_resid = bnorm > 0 ? maxpy<double>(c, b, 1.0, {}, {}, true) / bnorm : 0.0;
+  // weights A (into b, m fields) and B; real-space sums
+  k_grad_weights<<<nb, 256, 0, c->stream>>>(G, T, c->v64, uc, y, pd.beta, pd.closure, c->d_charge, rhoh3b, rhoh3,
+                                            b, Bw);
+  CKL();
+  const int n = c->n;
+  std::vector<double> gq(n, 0.0), gs(n, 0.0), ge(n, 0.0), gx(3 * (size_t)n, 0.0);
+  if (n > 0) {
+    const int rb = (int)std::min<long long>(2 * 148, (G.Nr + 255) / 256);
+    double *part = dalloc<double>((size_t)rb * n * 6);
+    k_grad_real<<<dim3(rb, n), 256, 0, c->stream>>>(G, h0, h1, h2, pd.L[0], pd.L[1], pd.L[2], c->d_solvent,
+                                                    c->d_solute, b, Bw, part);
+    CKL();
+    std::vector<double> hp((size_t)rb * n * 6);
+    CK(cudaMemcpyAsync(hp.data(), part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, c->stream));
+    // tau term: FFT lambda, then the half-spectrum sums
+    fwd3d(c, lam);
+    const long long nk = (long long)G.Nh * G.N1 * G.N2;
+    const int kb = (int)std::min<long long>(2 * 148, (nk + 255) / 256);
+    double *kpart = dalloc<double>((size_t)kb * n * 4);
+    k_grad_kspace<<<dim3(kb, n), 256, 0, c->stream>>>(G, c->work<double>(), c->s64, pd.nrad, c->dkr, c->d_solute,
+                                                      kpart);
+    CKL();
+    std::vector<double> hk((size_t)kb * n * 4);
+    CK(cudaMemcpyAsync(hk.data(), kpart, sizeof(double) * hk.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    dfree(part);
+    dfree(kpart);
+    const double kf = 1.0 / ((double)G.Nr * c->h3);
+    for (int u = 0; u < n; ++u) {
+      double a[6] = {0, 0, 0, 0, 0, 0}, k4[4] = {0, 0, 0, 0};
+      for (int q = 0; q < rb; ++q)
+        for (int j = 0; j < 6; ++j) a[j] += hp[((size_t)u * rb + q) * 6 + j];
+      for (int q = 0; q < kb; ++q)
+        for (int j = 0; j < 4; ++j) k4[j] += hk[((size_t)u * kb + q) * 4 + j];
+      gq[u] = a[0] + kf * k4[0];
+      gs[u] = a[1];
+      ge[u] = a[2];
+      for (int j = 0; j < 3; ++j) gx[3 * (size_t)u + j] = a[3 + j] + kf * k4[1 + j];
+    }
+  }
+  CK(cudaEventRecord(e1, c->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  gr->seconds = ms * 1e-3;
+  for (double *p : {b, y, w, Bw, uc, ones}) dfree(p);
+  if (gr->dq) std::copy(gq.begin(), gq.end(), gr->dq);
+  if (gr->dsigma) std::copy(gs.begin(), gs.end(), gr->dsigma);
+  if (gr->depsilon) std::copy(ge.begin(), ge.end(), gr->depsilon);
+  if (gr->dx) std::copy(gx.begin(), gx.end(), gr->dx);
+  return RISM3D_OK;
+}
+
 int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int n, const rism3d_site *solute,
                 const double *chi, rism3d_ctx **out) {
   if (!pd || !solvent || (!solute && n > 0) || !chi || !out) throw ArgFail{RISM3D_ERR_ARG, "null argument"};
@@ -1330,7 +1488,7 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
                     solvent[i].charge};
     c->d_solute = dalloc<SiteP>(std::max(n, 1));
     CK(cudaMemcpy(c->d_solute, hs.data(), sizeof(SiteP) * std::max(n, 1), cudaMemcpyHostToDevice));
-    SiteP *d_solvent = dalloc<SiteP>(m);
+    SiteP *d_solvent = c->d_solvent = dalloc<SiteP>(m);
     CK(cudaMemcpy(d_solvent, hv.data(), sizeof(SiteP) * m, cudaMemcpyHostToDevice));
     c->d_charge = dalloc<double>(m);
     CK(cudaMemcpy(c->d_charge, c->charge.data(), sizeof(double) * m, cudaMemcpyHostToDevice));
@@ -1352,7 +1510,6 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
                                                        c->L32);
     CKL();
     CK(cudaStreamSynchronize(cudaStreamPerThread));
-    dfree(d_solvent);
     c->W = dalloc<double2>((size_t)m * G.Nc);
     // reduction blocks: about four 16-byte loads per thread, at most 4 per SM
     c->red_blocks = (int)std::min<long long>(592, std::max<long long>(8, (c->nvec / 4 + 1023) / 1024));
@@ -1397,6 +1554,10 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
     allow((const void *)k_xfwd<float, MODE_J>);
     allow((const void *)k_xinv<double>);
     allow((const void *)k_xinv<float>);
+    allow((const void *)k_xfwd<double, MODE_FWD>);  // forward transform of the gradient
+    allow((const void *)k_z<double, MODE_FWD, 16>);
+    allow((const void *)k_z<double, MODE_FWD, 8>);
+    allow((const void *)k_z<double, MODE_FWD, 4>);
 #define OPTIN_YZ(T)                                  \
   allow((const void *)k_y<T, false, 16>);            \
   allow((const void *)k_y<T, true, 16>);             \
@@ -1694,6 +1855,50 @@ int rism3d_solve_batch(int m, const rism3d_site *solvent, int njobs, rism3d_job 
   for (auto &t : pool) t.join();
   int rc = RISM3D_OK;
   for (int i = 0; i < njobs && rc == RISM3D_OK; ++i) rc = jobs[i].result.status;
+  return rc;
+}
+
+int rism3d_jacobian_transpose_t1(rism3d_ctx *ctx, const double *T, const double *dT, double *JT) {
+  if (!ctx || !T || !dT || !JT) return RISM3D_ERR_ARG;
+  return guard([&] { return jacobian_transpose_impl(ctx, T, dT, JT); });
+}
+
+int rism3d_gradient(rism3d_ctx *ctx, const double *T, rism3d_grad *grad) {
+  if (!ctx || !T || !grad) return RISM3D_ERR_ARG;
+  return guard([&] { return gradient_impl(ctx, T, grad); });
+}
+
+int rism3d_solute_grad(const rism3d_problem *pd, int m, const rism3d_site *solvent, int n,
+                       const rism3d_site *solute, const double *chi, double *t_inout, rism3d_result *out,
+                       rism3d_grad *grad) {
+  if (!grad) return RISM3D_ERR_ARG;
+  if (pd && !pd->renorm) {
+    g_last_error = "the gradient is implemented for the renormalised form only";
+    return RISM3D_ERR_UNSUPPORTED;
+  }
+  rism3d_ctx *ctx = nullptr;
+  int rc = rism3d_ctx_create(pd, m, solvent, n, solute, chi, &ctx);
+  if (rc != RISM3D_OK) {
+    if (out) { std::memset(out, 0, sizeof(*out)); out->status = rc; }
+    return rc;
+  }
+  rc = guard([&] {
+    const size_t bytes = sizeof(double) * ctx->nvec;
+    double *T = dalloc<double>(ctx->nvec);
+    struct Free { double *a; ~Free() { dfree(a); } } fr{T};
+    if (t_inout) CK(cudaMemcpy(T, t_inout, bytes, cudaMemcpyHostToDevice));
+    else CK(cudaMemset(T, 0, bytes));
+    rism3d_result r{};
+    int st = solve_impl(ctx, T, &r);
+    observables_impl(ctx, T, nullptr, &r);
+    r.status = st;
+    if (st == RISM3D_OK) st = gradient_impl(ctx, T, grad);
+    if (t_inout) CK(cudaMemcpy(t_inout, T, bytes, cudaMemcpyDeviceToHost));
+    if (out) *out = r;
+    return st;
+  });
+  rism3d_ctx_destroy(ctx);
+  if (out && rc < 0 && out->status == 0) out->status = rc;
   return rc;
 }
 

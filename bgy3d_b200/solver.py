@@ -151,6 +151,45 @@ def hnc3d_run_solute(solute, solvent, settings, chi, restart=None, want_g=True, 
     return out
 
 
+def _grad_struct(n):
+    arrs = {k: np.zeros(n) for k in ("charge", "sigma", "epsilon")}
+    arrs["x"] = np.zeros((n, 3))
+    g = _abi.Grad()
+    g.dq, g.dsigma, g.depsilon, g.dx = (_dptr(arrs[k]) for k in ("charge", "sigma", "epsilon", "x"))
+    return g, arrs
+
+
+def _grad_dict(g, arrs):
+    return dict(arrs, **{"adjoint-jv": g.adjoint_jv, "adjoint-resid": g.adjoint_resid, "seconds": g.seconds})
+
+
+def hnc3d_solute_grad(solute, solvent, settings, chi, restart=None):
+    """Solve, then the free-energy gradient (rism3d_solute_grad): the result
+    dict of hnc3d_run_solute (no GUV) with "gradient" = {"charge": dmu/dq
+    [n], "sigma": [n], "epsilon": [n], "x": dmu/dx [n][3] (minus the
+    solvation force), "adjoint-jv", "adjoint-resid", "seconds"}."""
+    L = _abi.lib()
+    pd = problem_data(settings)
+    m, n = len(solvent), len(solute)
+    chi = np.ascontiguousarray(chi, dtype=np.float64)
+    if chi.shape != (m, m, pd.nrad):
+        raise ValueError(f"chi must be [{m}][{m}][{pd.nrad}], got {chi.shape}")
+    shape = (m, pd.N[2], pd.N[1], pd.N[0])
+    t = None if restart is None else np.array(restart, dtype=np.float64, order="C", copy=True)
+    if t is not None and t.shape != shape:
+        raise ValueError("restart has the wrong shape")
+    res = _abi.Result()
+    g, arrs = _grad_struct(n)
+    rc = L.rism3d_solute_grad(ctypes.byref(pd), m, _sites(solvent), n, _sites(solute), _dptr(chi),
+                              _dptr(t) if t is not None else None, ctypes.byref(res), ctypes.byref(g))
+    if rc != _abi.OK:
+        raise _abi.RismError(rc, "hnc3d_solute_grad")
+    out = _result_dict(res)
+    out["gradient"] = _grad_dict(g, arrs)
+    out["RESTART"] = t
+    return out
+
+
 def hnc3d_run_batch(solutes, solvent, settings, chi, workers=0, want_g=False, restarts=None):
     """Many solute solves in one solvent (rism3d_solve_batch), concurrently.
 
@@ -286,6 +325,22 @@ class RismContext:
         if rc not in (_abi.OK, _abi.ERR_NOT_CONVERGED, _abi.ERR_NAN):
             raise _abi.RismError(rc, "rism3d_solve")
         return T, _result_dict(res)
+
+    def jacobian_transpose_t1(self, T, dT, out=None):
+        """J(T)^T dT = c'(T) . ((chi-1) * dT) - dT (FP64)."""
+        t = self._torch
+        out = t.empty_like(dT) if out is None else out
+        _abi.check(_abi.lib().rism3d_jacobian_transpose_t1(self._h, self._check_vec(T, t.float64),
+                                                          self._check_vec(dT, t.float64),
+                                                          self._check_vec(out, t.float64)), "jacobian_transpose_t1")
+        return out
+
+    def gradient(self, T):
+        """dmu/d(solute q, sigma, eps, x) at a converged FP64 T (rism3d_gradient)."""
+        g, arrs = _grad_struct(self.n)
+        _abi.check(_abi.lib().rism3d_gradient(self._h, self._check_vec(T, self._torch.float64), ctypes.byref(g)),
+                   "gradient")
+        return _grad_dict(g, arrs)
 
     def observables(self, T, want_g=False):
         res = _abi.Result()

@@ -141,6 +141,37 @@ int rism3d_solute_solve(const rism3d_problem *pd,
                         double *t_inout, double *g_out,
                         rism3d_result *out);
 
+/* Derivatives of the free energy mu (the closure's native functional) with
+   respect to the solute's site parameters, and diagnostics of the adjoint
+   solve that yields them.  Arrays are host, caller-owned; a NULL array is
+   skipped.  Units: kcal/mol per e, per A (sigma, x), per kcal/mol (eps). */
+typedef struct rism3d_grad {
+  double *dq;         /* [n] dmu/dq_u */
+  double *dsigma;     /* [n] dmu/dsigma_u */
+  double *depsilon;   /* [n] dmu/depsilon_u */
+  double *dx;         /* [n][3] dmu/dx_u: minus the solvation force on site u */
+  int adjoint_jv;     /* J.v products of the adjoint solve */
+  double adjoint_resid; /* ||J^T lambda - dmu/dt||_2 / ||dmu/dt||_2 */
+  double seconds;     /* device time of the gradient */
+} rism3d_grad;
+
+/*
+  Solve, then dmu/d(solute q, sigma, eps, x).  Replaces the `derivatives`
+  branch of hnc3d_solute_solve (gradients / energy1 / field1,
+  hnc3d.c:1665-1742, bgy3d-solutes.c:381-468), which takes
+  dmu/dx = rho h^3 sum_i <g_i, dv_i/dx> (bgy3d-force.c forces), by the
+  adjoint of the converged fixed point instead: J^T lambda = dmu/dt, then
+  dmu/dp = d mu/dp|_t - lambda . dF/dp|_t, exact for any closure's
+  functional and for the renormalised long-range term.  Arguments as
+  rism3d_solute_solve (t_inout may be NULL).  Renormalised form only
+  (RISM3D_ERR_UNSUPPORTED with renorm = 0).
+*/
+int rism3d_solute_grad(const rism3d_problem *pd,
+                       int m, const rism3d_site *solvent,
+                       int n, const rism3d_site *solute,
+                       const double *chi, double *t_inout,
+                       rism3d_result *out, rism3d_grad *grad);
+
 /* One solute of a batch: the arguments of rism3d_solute_solve for that
    solute (its own problem -- grid, box, closure, precision -- and chi
    table) and its result. */
@@ -225,6 +256,14 @@ const char *rism3d_last_error(void);
    FP32 GMRES from zero.  Device pointers, FP64 [m][N2][N1][N0].  Returns
    RISM3D_ERR_UNSUPPORTED when the context has no coarse grid. */
 int rism3d_precondition(rism3d_ctx *ctx, const double *T, const double *v, double *z);
+
+/* The transposed Jacobian at T (the adjoint operator of the gradient):
+   JT = J^T dT = c'(T) . ((chi - 1) * dT) - dT.  FP64 device pointers. */
+int rism3d_jacobian_transpose_t1(rism3d_ctx *ctx, const double *T, const double *dT, double *JT);
+
+/* dmu/d(solute parameters) at a converged T (FP64 device pointer); see
+   rism3d_solute_grad. */
+int rism3d_gradient(rism3d_ctx *ctx, const double *T, rism3d_grad *grad);
 
 /* Points per axis of the two-grid preconditioner's coarse grid, written to
    n[3] (zeros when the preconditioner is off). */
