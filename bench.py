@@ -21,6 +21,12 @@ the reference's algorithm (the reference itself cannot be built here) on a
 bounded sample of residual and Jacobian evaluations, scaled by the number
 of evaluations the plain FP64 solve takes.
 
+Beside the timed line (unless --no-extras): "batch", 64 solutes of 3-40
+sites on grids 64^3..192^3 solved by rism3d_solve_batch in mixed and FP64
+precision (aggregate solves/s, per-solute |dmu|); "gradient", the adjoint
+dmu/d(q, sigma, eps, x) of the workload's solute (time against one
+solve, central-difference checks).
+
   python bench.py --profile-solve   one warm mixed solve between
                                     cudaProfilerStart/Stop (for ncu
                                     --profile-from-start off)
@@ -59,6 +65,90 @@ def workload(grid=GRID):
     s = dict(SETTINGS, N=grid)
     chi = rism_solvent(solvent, dict(s, **{"norm-tol": 1e-12}))["susceptibility"]
     return solute, solvent, s, chi
+
+
+BATCH_GRIDS = [64, 72, 96, 108, 128, 144, 162, 192]
+
+
+def batch_workload(count=64, s=None):
+    """Many-solute batch: solute i has n ~ U{3..40} sites drawn as the main
+    workload's (seed 20261203 + i, 6 A ball), half edge L = extent + 16 A
+    (extent = largest site distance from the centroid) and a grid drawn
+    from the even 2^a 3^b set 64..192 (seeded PCG64)."""
+    from bgy3d_b200 import synthetic_solute
+    rng = np.random.Generator(np.random.PCG64(20261203))
+    solutes, sets = [], []
+    for i in range(count):
+        n = int(rng.integers(3, 41))
+        sol = synthetic_solute(n, radius=6.0, seed=20261203 + i)
+        x = np.array([a["x"] for a in sol])
+        ext = float(np.max(np.linalg.norm(x - x.mean(axis=0), axis=1)))
+        solutes.append(sol)
+        sets.append(dict(s, N=int(rng.choice(BATCH_GRIDS)), L=ext + 16.0))
+    return solutes, sets
+
+
+def run_batch_report(solvent, s, chi, count=64, workers=8):
+    """Config of many solutes: aggregate solves/s of the mixed batch and of
+    the FP64 batch, per-solute |dmu| mixed vs FP64."""
+    import torch
+    from bgy3d_b200 import hnc3d_run_batch
+    solutes, sets = batch_workload(count, s)
+    out = {}
+    mus = {}
+    for prec in ("mixed", "fp64"):
+        st = [dict(x, precision=prec) for x in sets]
+        hnc3d_run_batch(solutes[:workers], solvent, st[:workers], chi, workers=workers)  # warm
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = hnc3d_run_batch(solutes, solvent, st, chi, workers=workers)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        ok = sum(r["status"] == 0 for r in res)
+        mus[prec] = np.array([r["free-energy"] for r in res])
+        out[prec] = {"solves_per_s": count / dt, "seconds": dt, "converged": ok,
+                     "launches": int(sum(r["launches"] for r in res))}
+    dmu = np.abs(mus["mixed"] - mus["fp64"])
+    out.update({"solutes": count, "workers": workers, "grids": BATCH_GRIDS,
+                "sites": [len(x) for x in solutes][:8] + ["..."],
+                "dmu_max": float(dmu.max()), "dmu_median": float(np.median(dmu)),
+                "timing": "host clock around rism3d_solve_batch, setup and teardown of every solve included"})
+    return out
+
+
+def run_gradient_report(solute, solvent, s, chi, ms_solve):
+    """Adjoint gradient of the main workload: time per gradient against the
+    forward solve, and central differences (h = 1e-4, FP64 solves) for four
+    parameters."""
+    from bgy3d_b200 import RismContext, hnc3d_run_solute
+    ctx = RismContext(solute, solvent, dict(s, precision="mixed"), chi)
+    T, res = ctx.solve()
+    ctx.gradient(T)  # warm
+    g = ctx.gradient(T)
+    ctx.close()
+    h = 1e-4
+    s64 = dict(s, precision="fp64", **{"norm-tol": 1e-12})
+    t_host = T.cpu().numpy()
+    checks = []
+    for u, key, val in ((0, "charge", g["charge"][0]), (1, "sigma", g["sigma"][1]),
+                        (2, "epsilon", g["epsilon"][2]), (3, "x", g["x"][3][0])):
+        mu = []
+        for sgn in (1, -1):
+            sol = [dict(a) for a in solute]
+            if key == "x":
+                x = list(sol[u]["x"])
+                x[0] += sgn * h
+                sol[u]["x"] = tuple(x)
+            else:
+                sol[u][key] += sgn * h
+            mu.append(hnc3d_run_solute(sol, solvent, s64, chi, restart=t_host, want_g=False)["free-energy"])
+        fd = (mu[0] - mu[1]) / (2 * h)
+        checks.append({"site": u, "param": key, "adjoint": val, "central_difference": fd,
+                       "rel_err": abs(val - fd) / max(abs(fd), 1e-12)})
+    return {"seconds_per_gradient": g["seconds"], "seconds_per_solve": ms_solve * 1e-3,
+            "gradient_over_solve": g["seconds"] / (ms_solve * 1e-3), "adjoint_jv": g["adjoint-jv"],
+            "adjoint_resid": g["adjoint-resid"], "fd_checks": checks,
+            "params": "dmu/d{q, sigma, eps, x} of all %d sites" % len(solute)}
 
 
 def config(grid=GRID, precision="mixed"):
@@ -260,6 +350,9 @@ def run_ours(args, rank, world):
         line["clocks"] = clocks
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, sample_evals=1)
+    if world == 1 and not args.no_extras:
+        line["batch"] = run_batch_report(solvent, s, chi)
+        line["gradient"] = run_gradient_report(solute, solvent, s, chi, ms / args.steps)
     return line
 
 
@@ -379,6 +472,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--grid", type=int, default=GRID)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the many-solute batch and gradient reports")
     ap.add_argument("--evals", type=int, default=0,
                     help="profiling mode: time this many F and J.v evaluations instead of solves")
     ap.add_argument("--profile-solve", action="store_true",
