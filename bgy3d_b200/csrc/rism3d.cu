@@ -353,8 +353,8 @@ template <typename T, int N> constexpr size_t ys_smem() {
 template <typename T, int N> size_t zs_smem(int m) {
   return sizeof(typename Cx<T>::type) * (size_t)(m * N * static_Bz<T>() + N) + 16;
 }
-bool static_len_x(int M) { return M == 48 || M == 64 || M == 128; }
-bool static_len_yz(int N) { return N == 96 || N == 128 || N == 256; }
+bool static_len_x(int M) { return M == 24 || M == 48 || M == 64 || M == 128; }
+bool static_len_yz(int N) { return N == 48 || N == 96 || N == 128 || N == 256; }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {  // thread-safe one-time lookup
@@ -404,7 +404,7 @@ template <typename T, bool INV> void launch_y(rism3d_ctx *c) {
   case N:                                                                                           \
     k_y_s<T, INV, N, B><<<grid, Split<N>::R1 * B, ys_smem<T, N>(), c->stream>>>(c->g, tm, tw, c->d_err); \
     break;
-      Y_CASE(96) Y_CASE(128) Y_CASE(256)
+      Y_CASE(48) Y_CASE(96) Y_CASE(128) Y_CASE(256)
 #undef Y_CASE
     }
     CKL();
@@ -433,7 +433,7 @@ template <typename T, int MODE> void launch_z(rism3d_ctx *c) {
     k_z_s<T, MODE, N, B, 3><<<grid, Split<N>::R1 * B, zs_smem<T, N>(c->m), c->stream>>>(c->g, tm, tw, zp, \
                                                                                           c->d_err);     \
     break;
-      Z_CASE(96) Z_CASE(128) Z_CASE(256)
+      Z_CASE(48) Z_CASE(96) Z_CASE(128) Z_CASE(256)
 #undef Z_CASE
     }
     CKL();
@@ -488,7 +488,7 @@ int pipeline(rism3d_ctx *c, const T *A, const T *Bv, T p, T sub, T *out) {
     k_xfwd_s<T, MODE, M, kStaticRX><<<gx, 256, xs_smem<T, M>(), c->stream>>>(c->g, A, Bv, p, c->pd.closure, \
                                                                              W, postw<T>(c), twx);      \
     break;
-        XF_CASE(48) XF_CASE(64) XF_CASE(128)
+        XF_CASE(24) XF_CASE(48) XF_CASE(64) XF_CASE(128)
 #undef XF_CASE
       }
     } else {
@@ -510,7 +510,7 @@ int pipeline(rism3d_ctx *c, const T *A, const T *Bv, T p, T sub, T *out) {
     k_xinv_s<T, M, kStaticRX><<<gx, 256, xs_smem<T, M>(), c->stream>>>(c->g, W, A, out, scale, sub, postw<T>(c), \
                                                                        twx, c->npart);                        \
     break;
-        XI_CASE(48) XI_CASE(64) XI_CASE(128)
+        XI_CASE(24) XI_CASE(48) XI_CASE(64) XI_CASE(128)
 #undef XI_CASE
       }
     } else {
@@ -1578,6 +1578,13 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
       need = std::max({xs_smem<double, 128>(), ys_smem<double, 256>(), zs_smem<double, 256>(m),
                        xs_smem<float, 128>(), ys_smem<float, 256>(), zs_smem<float, 256>(m)});
 #define OPTIN_S(T)                                                                          \
+  allow((const void *)k_xfwd_s<T, MODE_F, 24, kStaticRX>);                                  \
+  allow((const void *)k_xfwd_s<T, MODE_J, 24, kStaticRX>);                                  \
+  allow((const void *)k_xinv_s<T, 24, kStaticRX>);                                          \
+  allow((const void *)k_y_s<T, false, 48, static_B<T>()>);                                  \
+  allow((const void *)k_y_s<T, true, 48, static_B<T>()>);                                   \
+  allow((const void *)k_z_s<T, MODE_F, 48, static_Bz<T>(), 3>);                              \
+  allow((const void *)k_z_s<T, MODE_J, 48, static_Bz<T>(), 3>);                              \
   allow((const void *)k_xfwd_s<T, MODE_F, 48, kStaticRX>);                                  \
   allow((const void *)k_xfwd_s<T, MODE_J, 48, kStaticRX>);                                  \
   allow((const void *)k_xfwd_s<T, MODE_F, 64, kStaticRX>);                                  \
