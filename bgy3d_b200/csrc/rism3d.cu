@@ -353,8 +353,15 @@ template <typename T, int N> constexpr size_t ys_smem() {
 template <typename T, int N> size_t zs_smem(int m) {
   return sizeof(typename Cx<T>::type) * (size_t)(m * N * static_Bz<T>() + N) + 16;
 }
-bool static_len_x(int M) { return M == 24 || M == 48 || M == 64 || M == 128; }
-bool static_len_yz(int N) { return N == 48 || N == 96 || N == 128 || N == 256; }
+// Lengths with shape-specialised passes: the coarse grids (48, 96) and the
+// even 2^a 3^b grids of the many-solute workloads whose two-step split fits
+// the register transforms (108 and 162 do not: no split of 54 / odd 81).
+bool static_len_x(int M) {
+  return M == 24 || M == 32 || M == 36 || M == 48 || M == 64 || M == 72 || M == 96 || M == 128;
+}
+bool static_len_yz(int N) {
+  return N == 48 || N == 64 || N == 72 || N == 96 || N == 128 || N == 144 || N == 192 || N == 256;
+}
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {  // thread-safe one-time lookup
@@ -404,7 +411,7 @@ template <typename T, bool INV> void launch_y(rism3d_ctx *c) {
   case N:                                                                                           \
     k_y_s<T, INV, N, B><<<grid, Split<N>::R1 * B, ys_smem<T, N>(), c->stream>>>(c->g, tm, tw, c->d_err); \
     break;
-      Y_CASE(48) Y_CASE(96) Y_CASE(128) Y_CASE(256)
+      Y_CASE(48) Y_CASE(64) Y_CASE(72) Y_CASE(96) Y_CASE(128) Y_CASE(144) Y_CASE(192) Y_CASE(256)
 #undef Y_CASE
     }
     CKL();
@@ -433,7 +440,7 @@ template <typename T, int MODE> void launch_z(rism3d_ctx *c) {
     k_z_s<T, MODE, N, B, 3><<<grid, Split<N>::R1 * B, zs_smem<T, N>(c->m), c->stream>>>(c->g, tm, tw, zp, \
                                                                                           c->d_err);     \
     break;
-      Z_CASE(48) Z_CASE(96) Z_CASE(128) Z_CASE(256)
+      Z_CASE(48) Z_CASE(64) Z_CASE(72) Z_CASE(96) Z_CASE(128) Z_CASE(144) Z_CASE(192) Z_CASE(256)
 #undef Z_CASE
     }
     CKL();
@@ -488,7 +495,7 @@ int pipeline(rism3d_ctx *c, const T *A, const T *Bv, T p, T sub, T *out) {
     k_xfwd_s<T, MODE, M, kStaticRX><<<gx, 256, xs_smem<T, M>(), c->stream>>>(c->g, A, Bv, p, c->pd.closure, \
                                                                              W, postw<T>(c), twx);      \
     break;
-        XF_CASE(24) XF_CASE(48) XF_CASE(64) XF_CASE(128)
+        XF_CASE(24) XF_CASE(32) XF_CASE(36) XF_CASE(48) XF_CASE(64) XF_CASE(72) XF_CASE(96) XF_CASE(128)
 #undef XF_CASE
       }
     } else {
@@ -510,7 +517,7 @@ int pipeline(rism3d_ctx *c, const T *A, const T *Bv, T p, T sub, T *out) {
     k_xinv_s<T, M, kStaticRX><<<gx, 256, xs_smem<T, M>(), c->stream>>>(c->g, W, A, out, scale, sub, postw<T>(c), \
                                                                        twx, c->npart);                        \
     break;
-        XI_CASE(24) XI_CASE(48) XI_CASE(64) XI_CASE(128)
+        XI_CASE(24) XI_CASE(32) XI_CASE(36) XI_CASE(48) XI_CASE(64) XI_CASE(72) XI_CASE(96) XI_CASE(128)
 #undef XI_CASE
       }
     } else {
@@ -1577,34 +1584,62 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
     if (c->stat[0]) {
       need = std::max({xs_smem<double, 128>(), ys_smem<double, 256>(), zs_smem<double, 256>(m),
                        xs_smem<float, 128>(), ys_smem<float, 256>(), zs_smem<float, 256>(m)});
-#define OPTIN_S(T)                                                                          \
-  allow((const void *)k_xfwd_s<T, MODE_F, 24, kStaticRX>);                                  \
-  allow((const void *)k_xfwd_s<T, MODE_J, 24, kStaticRX>);                                  \
-  allow((const void *)k_xinv_s<T, 24, kStaticRX>);                                          \
-  allow((const void *)k_y_s<T, false, 48, static_B<T>()>);                                  \
-  allow((const void *)k_y_s<T, true, 48, static_B<T>()>);                                   \
-  allow((const void *)k_z_s<T, MODE_F, 48, static_Bz<T>(), 3>);                              \
-  allow((const void *)k_z_s<T, MODE_J, 48, static_Bz<T>(), 3>);                              \
-  allow((const void *)k_xfwd_s<T, MODE_F, 48, kStaticRX>);                                  \
-  allow((const void *)k_xfwd_s<T, MODE_J, 48, kStaticRX>);                                  \
-  allow((const void *)k_xfwd_s<T, MODE_F, 64, kStaticRX>);                                  \
-  allow((const void *)k_xfwd_s<T, MODE_J, 64, kStaticRX>);                                  \
-  allow((const void *)k_xfwd_s<T, MODE_F, 128, kStaticRX>);                                 \
-  allow((const void *)k_xfwd_s<T, MODE_J, 128, kStaticRX>);                                 \
-  allow((const void *)k_xinv_s<T, 48, kStaticRX>);                                          \
-  allow((const void *)k_xinv_s<T, 64, kStaticRX>);                                          \
-  allow((const void *)k_xinv_s<T, 128, kStaticRX>);                                         \
-  allow((const void *)k_y_s<T, false, 96, static_B<T>()>);                                  \
-  allow((const void *)k_y_s<T, true, 96, static_B<T>()>);                                   \
-  allow((const void *)k_y_s<T, false, 128, static_B<T>()>);                                 \
-  allow((const void *)k_y_s<T, true, 128, static_B<T>()>);                                  \
-  allow((const void *)k_y_s<T, false, 256, static_B<T>()>);                                 \
-  allow((const void *)k_y_s<T, true, 256, static_B<T>()>);                                  \
-  allow((const void *)k_z_s<T, MODE_F, 96, static_Bz<T>(), 3>);                              \
-  allow((const void *)k_z_s<T, MODE_J, 96, static_Bz<T>(), 3>);                              \
-  allow((const void *)k_z_s<T, MODE_F, 128, static_Bz<T>(), 3>);                             \
-  allow((const void *)k_z_s<T, MODE_J, 128, static_Bz<T>(), 3>);                             \
-  allow((const void *)k_z_s<T, MODE_F, 256, static_Bz<T>(), 3>);                             \
+#define OPTIN_S(T)                                               \
+  allow((const void *)k_xfwd_s<T, MODE_F, 24, kStaticRX>);       \
+  allow((const void *)k_xfwd_s<T, MODE_J, 24, kStaticRX>);       \
+  allow((const void *)k_xinv_s<T, 24, kStaticRX>);               \
+  allow((const void *)k_xfwd_s<T, MODE_F, 32, kStaticRX>);       \
+  allow((const void *)k_xfwd_s<T, MODE_J, 32, kStaticRX>);       \
+  allow((const void *)k_xinv_s<T, 32, kStaticRX>);               \
+  allow((const void *)k_xfwd_s<T, MODE_F, 36, kStaticRX>);       \
+  allow((const void *)k_xfwd_s<T, MODE_J, 36, kStaticRX>);       \
+  allow((const void *)k_xinv_s<T, 36, kStaticRX>);               \
+  allow((const void *)k_xfwd_s<T, MODE_F, 48, kStaticRX>);       \
+  allow((const void *)k_xfwd_s<T, MODE_J, 48, kStaticRX>);       \
+  allow((const void *)k_xinv_s<T, 48, kStaticRX>);               \
+  allow((const void *)k_xfwd_s<T, MODE_F, 64, kStaticRX>);       \
+  allow((const void *)k_xfwd_s<T, MODE_J, 64, kStaticRX>);       \
+  allow((const void *)k_xinv_s<T, 64, kStaticRX>);               \
+  allow((const void *)k_xfwd_s<T, MODE_F, 72, kStaticRX>);       \
+  allow((const void *)k_xfwd_s<T, MODE_J, 72, kStaticRX>);       \
+  allow((const void *)k_xinv_s<T, 72, kStaticRX>);               \
+  allow((const void *)k_xfwd_s<T, MODE_F, 96, kStaticRX>);       \
+  allow((const void *)k_xfwd_s<T, MODE_J, 96, kStaticRX>);       \
+  allow((const void *)k_xinv_s<T, 96, kStaticRX>);               \
+  allow((const void *)k_xfwd_s<T, MODE_F, 128, kStaticRX>);      \
+  allow((const void *)k_xfwd_s<T, MODE_J, 128, kStaticRX>);      \
+  allow((const void *)k_xinv_s<T, 128, kStaticRX>);              \
+  allow((const void *)k_y_s<T, false, 48, static_B<T>()>);       \
+  allow((const void *)k_y_s<T, true, 48, static_B<T>()>);        \
+  allow((const void *)k_z_s<T, MODE_F, 48, static_Bz<T>(), 3>);  \
+  allow((const void *)k_z_s<T, MODE_J, 48, static_Bz<T>(), 3>);  \
+  allow((const void *)k_y_s<T, false, 64, static_B<T>()>);       \
+  allow((const void *)k_y_s<T, true, 64, static_B<T>()>);        \
+  allow((const void *)k_z_s<T, MODE_F, 64, static_Bz<T>(), 3>);  \
+  allow((const void *)k_z_s<T, MODE_J, 64, static_Bz<T>(), 3>);  \
+  allow((const void *)k_y_s<T, false, 72, static_B<T>()>);       \
+  allow((const void *)k_y_s<T, true, 72, static_B<T>()>);        \
+  allow((const void *)k_z_s<T, MODE_F, 72, static_Bz<T>(), 3>);  \
+  allow((const void *)k_z_s<T, MODE_J, 72, static_Bz<T>(), 3>);  \
+  allow((const void *)k_y_s<T, false, 96, static_B<T>()>);       \
+  allow((const void *)k_y_s<T, true, 96, static_B<T>()>);        \
+  allow((const void *)k_z_s<T, MODE_F, 96, static_Bz<T>(), 3>);  \
+  allow((const void *)k_z_s<T, MODE_J, 96, static_Bz<T>(), 3>);  \
+  allow((const void *)k_y_s<T, false, 128, static_B<T>()>);      \
+  allow((const void *)k_y_s<T, true, 128, static_B<T>()>);       \
+  allow((const void *)k_z_s<T, MODE_F, 128, static_Bz<T>(), 3>); \
+  allow((const void *)k_z_s<T, MODE_J, 128, static_Bz<T>(), 3>); \
+  allow((const void *)k_y_s<T, false, 144, static_B<T>()>);      \
+  allow((const void *)k_y_s<T, true, 144, static_B<T>()>);       \
+  allow((const void *)k_z_s<T, MODE_F, 144, static_Bz<T>(), 3>); \
+  allow((const void *)k_z_s<T, MODE_J, 144, static_Bz<T>(), 3>); \
+  allow((const void *)k_y_s<T, false, 192, static_B<T>()>);      \
+  allow((const void *)k_y_s<T, true, 192, static_B<T>()>);       \
+  allow((const void *)k_z_s<T, MODE_F, 192, static_Bz<T>(), 3>); \
+  allow((const void *)k_z_s<T, MODE_J, 192, static_Bz<T>(), 3>); \
+  allow((const void *)k_y_s<T, false, 256, static_B<T>()>);      \
+  allow((const void *)k_y_s<T, true, 256, static_B<T>()>);       \
+  allow((const void *)k_z_s<T, MODE_F, 256, static_Bz<T>(), 3>); \
   allow((const void *)k_z_s<T, MODE_J, 256, static_Bz<T>(), 3>);
       OPTIN_S(double)
       OPTIN_S(float)

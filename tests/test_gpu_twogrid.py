@@ -5,7 +5,7 @@ coarse Jacobian J_H built from the restricted closure slope R c'(T), and a
 fixed-step GMRES for J_H^-1.  The GPU result is checked against a NumPy
 restatement on the oracle's operators at the coarse size; the coarse solve
 runs in FP32 on the GPU, so the tolerance is 1e-4 of max|z|.  The
-runtime-length FFT passes at the coarse sizes (16^3, 18^3, 48^3) are
+FFT passes at the coarse sizes and the many-solute grids (16^3 ... 192^3) are
 checked against the oracle at the usual 1e-11 (FP64) / 2e-5 (FP32), and
 solves with the preconditioner on, started from zero, reach the oracle's
 root.
@@ -29,9 +29,9 @@ def settings_of(meta, **kw):
     return s
 
 
-def problem(meta, chi, n):
+def problem(meta, chi, n, L=None):
     s = meta["settings"]
-    return hnc3d.Problem((n,) * 3, (2 * s["L"],) * 3, s["beta"], s["rho"], int(s["closure"]), meta["solvent"],
+    return hnc3d.Problem((n,) * 3, (2 * (L or s["L"]),) * 3, s["beta"], s["rho"], int(s["closure"]), meta["solvent"],
                          meta["solute"], chi, s["rmax"], renorm=not s["no-renorm"])
 
 
@@ -71,11 +71,13 @@ def gmres_steps(A, b, k):
     return sum(yi * v for yi, v in zip(y, V))
 
 
-@pytest.mark.parametrize("n", [16, 18, 48])
+@pytest.mark.parametrize("n", [16, 18, 48, 64, 72, 144, 192])
 def test_coarse_sizes_match_oracle(fixture_loader, n):
+    """Runtime-length passes (16, 18) and shape-specialised ones (the rest),
+    in a 48 A box so that |k| stays inside the fixture's chi table."""
     meta, arr = fixture_loader("water_hnc_n24")
-    ctx = RismContext(meta["solute"], meta["solvent"], settings_of(meta, N=n, **{"coarse-h": 0}), arr["chi"])
-    P = problem(meta, arr["chi"], n)
+    ctx = RismContext(meta["solute"], meta["solvent"], settings_of(meta, N=n, L=24.0, **{"coarse-h": 0}), arr["chi"])
+    P = problem(meta, arr["chi"], n, L=24.0)
     rng = np.random.default_rng(11)
     T = 0.3 * rng.standard_normal(ctx.shape)
     dT = rng.standard_normal(ctx.shape)
