@@ -20,15 +20,17 @@ namespace tg {
 // Restriction along x: out[row][i] = s * sum_j R[i][j] in[row][j]
 // (rows x N0 -> rows x Nc0), R given transposed: Rt[j][i] = R[i][j].
 // CTA tile 128 rows x 48 coarse columns, 128 threads, 8 x 6 outputs per
-// thread, K staged through shared memory in chunks of 32.
-constexpr int kRxRows = 128, kRxCols = 48, kRxK = 32, kRxThreads = 128;
+// thread, K staged through shared memory in chunks of 32; rows are padded to
+// a multiple of 4 floats so a thread's 8 rows load as two float4 and its 6
+// columns as three float2 (48 FMA per 5 shared loads).
+constexpr int kRxRows = 128, kRxCols = 48, kRxK = 32, kRxThreads = 128, kRxPad = kRxRows + 4;
 
 template <typename TI>
 __global__ void __launch_bounds__(kRxThreads) k_restrict_x(long long rows, int N, int Nc, const TI *__restrict__ in,
                                                           float s, const float *__restrict__ Rt,
                                                           float *__restrict__ out) {
-  __shared__ float Xs[kRxK][kRxRows + 1];
-  __shared__ float Rs[kRxK][kRxCols];
+  __shared__ __align__(16) float Xs[kRxK][kRxPad];
+  __shared__ __align__(16) float Rs[kRxK][kRxCols];
   const int t = threadIdx.x;
   const int tr = t >> 3, tc = t & 7;  // rows tr*8.., cols tc*6..
   const long long row0 = (long long)blockIdx.x * kRxRows;
@@ -54,11 +56,13 @@ __global__ void __launch_bounds__(kRxThreads) k_restrict_x(long long rows, int N
     __syncthreads();
 #pragma unroll 4
     for (int kk = 0; kk < kRxK; ++kk) {
-      float x[8], r[6];
-#pragma unroll
-      for (int a = 0; a < 8; ++a) x[a] = Xs[kk][tr * 8 + a];
-#pragma unroll
-      for (int b = 0; b < 6; ++b) r[b] = Rs[kk][tc * 6 + b];
+      const float4 x0 = *reinterpret_cast<const float4 *>(&Xs[kk][tr * 8]);
+      const float4 x1 = *reinterpret_cast<const float4 *>(&Xs[kk][tr * 8 + 4]);
+      const float2 r0 = *reinterpret_cast<const float2 *>(&Rs[kk][tc * 6]);
+      const float2 r1 = *reinterpret_cast<const float2 *>(&Rs[kk][tc * 6 + 2]);
+      const float2 r2 = *reinterpret_cast<const float2 *>(&Rs[kk][tc * 6 + 4]);
+      const float x[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+      const float r[6] = {r0.x, r0.y, r1.x, r1.y, r2.x, r2.y};
 #pragma unroll
       for (int a = 0; a < 8; ++a)
 #pragma unroll
@@ -82,15 +86,40 @@ __global__ void __launch_bounds__(kRxThreads) k_restrict_x(long long rows, int N
 // out[row][j] = sum_i P[j][i] y[row][i] - s * r[row][j]
 // (rows x Nc0 -> rows x N0), P given transposed: Pt[i][j] = P[j][i].
 // CTA tile 64 rows x 128 fine columns, 128 threads, 8 x 8 outputs per
-// thread; each thread writes 8 consecutive elements of a row, a warp
-// 16 x 8 consecutive ones.
-constexpr int kPxRows = 64, kPxCols = 128, kPxK = 16, kPxThreads = 128;
+// thread (64 FMA per four float4 shared loads); each thread reads r and
+// writes out as 8 consecutive elements of a row, a warp 16 x 8 of them.
+constexpr int kPxRows = 64, kPxCols = 128, kPxK = 16, kPxThreads = 128, kPxPad = kPxRows + 4;
+
+template <typename T> struct Vec8;
+template <> struct Vec8<float> {
+  __device__ __forceinline__ static void load(const float *p, float v[8]) {
+    const float4 a = reinterpret_cast<const float4 *>(p)[0], b = reinterpret_cast<const float4 *>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  }
+  __device__ __forceinline__ static void store(float *p, const float v[8]) {
+    reinterpret_cast<float4 *>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
+    reinterpret_cast<float4 *>(p)[1] = make_float4(v[4], v[5], v[6], v[7]);
+  }
+};
+template <> struct Vec8<double> {
+  __device__ __forceinline__ static void load(const double *p, double v[8]) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double2 a = reinterpret_cast<const double2 *>(p)[q];
+      v[2 * q] = a.x; v[2 * q + 1] = a.y;
+    }
+  }
+  __device__ __forceinline__ static void store(double *p, const double v[8]) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) reinterpret_cast<double2 *>(p)[q] = make_double2(v[2 * q], v[2 * q + 1]);
+  }
+};
 
 template <typename TO, typename TR>
 __global__ void __launch_bounds__(kPxThreads) k_prolong_x(long long rows, int N, int Nc, const float *__restrict__ y,
                                                          const float *__restrict__ Pt, const TR *__restrict__ r,
                                                          double s, TO *__restrict__ out) {
-  __shared__ float Ys[kPxK][kPxRows + 1];
+  __shared__ __align__(16) float Ys[kPxK][kPxPad];
   __shared__ __align__(16) float Ps[kPxK][kPxCols];
   const int t = threadIdx.x;
   const int tr = t >> 4, tc = t & 15;  // rows tr*8.., cols tc*8..
@@ -114,13 +143,12 @@ __global__ void __launch_bounds__(kPxThreads) k_prolong_x(long long rows, int N,
     __syncthreads();
 #pragma unroll 4
     for (int kk = 0; kk < kPxK; ++kk) {
-      float yv[8], pv[8];
-#pragma unroll
-      for (int a = 0; a < 8; ++a) yv[a] = Ys[kk][tr * 8 + a];
+      const float4 y0 = *reinterpret_cast<const float4 *>(&Ys[kk][tr * 8]);
+      const float4 y1 = *reinterpret_cast<const float4 *>(&Ys[kk][tr * 8 + 4]);
       const float4 p0 = *reinterpret_cast<const float4 *>(&Ps[kk][tc * 8]);
       const float4 p1 = *reinterpret_cast<const float4 *>(&Ps[kk][tc * 8 + 4]);
-      pv[0] = p0.x; pv[1] = p0.y; pv[2] = p0.z; pv[3] = p0.w;
-      pv[4] = p1.x; pv[5] = p1.y; pv[6] = p1.z; pv[7] = p1.w;
+      const float yv[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+      const float pv[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
 #pragma unroll
       for (int a = 0; a < 8; ++a)
 #pragma unroll
@@ -128,17 +156,24 @@ __global__ void __launch_bounds__(kPxThreads) k_prolong_x(long long rows, int N,
     }
     __syncthreads();
   }
+  const int c0 = col0 + tc * 8;
+  const bool full = c0 + 8 <= N && (N % 8) == 0;
 #pragma unroll
   for (int a = 0; a < 8; ++a) {
     const long long row = row0 + tr * 8 + a;
     if (row >= rows) continue;
+    const long long p = row * N + c0;
+    if (full) {
+      TR rv[8];
+      TO ov[8];
+      Vec8<TR>::load(r + p, rv);
 #pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      const int col = col0 + tc * 8 + b;
-      if (col < N) {
-        const long long p = row * N + col;
-        out[p] = (TO)((double)acc[a][b] - s * (double)r[p]);
-      }
+      for (int b = 0; b < 8; ++b) ov[b] = (TO)((double)acc[a][b] - s * (double)rv[b]);
+      Vec8<TO>::store(out + p, ov);
+    } else {
+#pragma unroll
+      for (int b = 0; b < 8; ++b)
+        if (c0 + b < N) out[p + b] = (TO)((double)acc[a][b] - s * (double)r[p + b]);
     }
   }
 }
