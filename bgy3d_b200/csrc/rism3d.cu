@@ -29,6 +29,7 @@
 #include "krylov.cuh"
 #include "rism3d.h"
 #include "twogrid.cuh"
+#include "twogrid_fft.cuh"
 
 using namespace rism;
 
@@ -222,6 +223,7 @@ struct rism3d_ctx {
   int Nc[3] = {0, 0, 0};
   float *tR[3] = {nullptr, nullptr, nullptr}, *tRt[3] = {nullptr, nullptr, nullptr};
   float *tP[3] = {nullptr, nullptr, nullptr}, *tPt[3] = {nullptr, nullptr, nullptr};
+  float2 *tC = nullptr, *tD = nullptr;     // x-axis FFT-transfer tables
   float *tA = nullptr, *tB = nullptr;       // partially transferred fields
   float *tc_r = nullptr, *tc_y = nullptr;   // coarse right-hand side / solution
   int coarse_jv = 0;
@@ -254,7 +256,7 @@ struct rism3d_ctx {
     for (auto p : zbasis64) fr(p);
     for (auto p : zbasis32) fr(p);
     for (int a = 0; a < 3; ++a) { fr(tR[a]); fr(tRt[a]); fr(tP[a]); fr(tPt[a]); }
-    fr(tA); fr(tB); fr(tc_r); fr(tc_y); fr(cg_H); fr(cg_aux);
+    fr(tA); fr(tB); fr(tc_r); fr(tc_y); fr(cg_H); fr(cg_aux); fr(tC); fr(tD);
     if (cg_exec) cudaGraphExecDestroy(cg_exec);
     if (cg_graph) cudaGraphDestroy(cg_graph);
     delete coarse;
@@ -769,13 +771,65 @@ void transfer_axis(rism3d_ctx *c, int outer, int n_in, int n_out, int inner, con
   CKL();
 }
 
+// x-axis transfers by FFT (twogrid_fft.cuh) where the row length has a
+// shape-specialised transform; false: use the dense tiles.
+constexpr int kFxRX = 16;
+bool fx_usable(const rism3d_ctx *c) {
+  return c->tC && static_len_x(c->g.M) && c->Nc[0] % 2 == 0 && c->Nc[0] / 2 < c->g.M;
+}
+template <typename T> bool fx_restrict(rism3d_ctx *c, long long rows, const T *in, double s) {
+  if (!fx_usable(c)) return false;
+  const int K = c->Nc[0] / 2;
+  const auto *post = postw<float>(c);
+  const auto *tw = static_cast<const float2 *>(c->plan<float>(0).tw);
+  const unsigned nb = (unsigned)((rows + kFxRX - 1) / kFxRX);
+  switch (c->g.M) {
+#define FXR(M)                                                                                                 \
+  case M: {                                                                                                    \
+    const size_t sm = fx_smem_restrict<M, kFxRX>(K, c->Nc[0]);                                                           \
+    if (sm > 48 * 1024) return false;                                                                         \
+    k_restrict_fx<T, M, kFxRX><<<nb, 256, sm, c->stream>>>(rows, c->Nc[0], K, in, (float)s, post, tw, c->tC, c->tA); \
+    break;                                                                                                     \
+  }
+    FXR(24) FXR(32) FXR(36) FXR(48) FXR(64) FXR(72) FXR(96) FXR(128)
+#undef FXR
+    default: return false;
+  }
+  CKL();
+  return true;
+}
+template <typename T> bool fx_prolong(rism3d_ctx *c, long long rows, const T *r, double s, T *out) {
+  if (!fx_usable(c)) return false;
+  const int K = c->Nc[0] / 2;
+  const auto *post = postw<float>(c);
+  const auto *tw = static_cast<const float2 *>(c->plan<float>(0).tw);
+  const unsigned nb = (unsigned)((rows + kFxRX - 1) / kFxRX);
+  switch (c->g.M) {
+#define FXP(M)                                                                                                 \
+  case M: {                                                                                                    \
+    const size_t sm = fx_smem_prolong<M, kFxRX>(K, c->Nc[0]);                                                  \
+    if (sm > 48 * 1024) return false;                                                                         \
+    k_prolong_fx<T, T, M, kFxRX><<<nb, 256, sm, c->stream>>>(rows, c->Nc[0], K, c->tA, post, tw, c->tD, r, s, out); \
+    break;                                                                                                     \
+  }
+    FXP(24) FXP(32) FXP(36) FXP(48) FXP(64) FXP(72) FXP(96) FXP(128)
+#undef FXP
+    default: return false;
+  }
+  CKL();
+  return true;
+}
+
 // out (coarse [m][Nc2][Nc1][Nc0]) = R (s in), in fine [m][N2][N1][N0].
 template <typename T> void tg_restrict(rism3d_ctx *c, const T *in, double s, float *out) {
   const Geo &G = c->g;
   const long long rows = (long long)c->m * G.N2 * G.N1;
-  dim3 gx((unsigned)((rows + tg::kRxRows - 1) / tg::kRxRows), (unsigned)((c->Nc[0] + tg::kRxCols - 1) / tg::kRxCols));
-  tg::k_restrict_x<T><<<gx, tg::kRxThreads, 0, c->stream>>>(rows, G.N0, c->Nc[0], in, (float)s, c->tRt[0], c->tA);
-  CKL();
+  if (!fx_restrict<T>(c, rows, in, s)) {
+    dim3 gx((unsigned)((rows + tg::kRxRows - 1) / tg::kRxRows),
+            (unsigned)((c->Nc[0] + tg::kRxCols - 1) / tg::kRxCols));
+    tg::k_restrict_x<T><<<gx, tg::kRxThreads, 0, c->stream>>>(rows, G.N0, c->Nc[0], in, (float)s, c->tRt[0], c->tA);
+    CKL();
+  }
   transfer_axis(c, c->m * G.N2, G.N1, c->Nc[1], c->Nc[0], c->tA, c->tR[1], c->tB);
   transfer_axis(c, c->m, G.N2, c->Nc[2], c->Nc[1] * c->Nc[0], c->tB, c->tR[2], out);
 }
@@ -786,9 +840,11 @@ template <typename T> void tg_prolong(rism3d_ctx *c, const float *yc, const T *r
   transfer_axis(c, c->m, c->Nc[2], G.N2, c->Nc[1] * c->Nc[0], yc, c->tP[2], c->tB);
   transfer_axis(c, c->m * G.N2, c->Nc[1], G.N1, c->Nc[0], c->tB, c->tP[1], c->tA);
   const long long rows = (long long)c->m * G.N2 * G.N1;
-  dim3 gx((unsigned)((rows + tg::kPxRows - 1) / tg::kPxRows), (unsigned)((G.N0 + tg::kPxCols - 1) / tg::kPxCols));
-  tg::k_prolong_x<T, T><<<gx, tg::kPxThreads, 0, c->stream>>>(rows, G.N0, c->Nc[0], c->tA, c->tPt[0], r, s, out);
-  CKL();
+  if (!fx_prolong<T>(c, rows, r, s, out)) {
+    dim3 gx((unsigned)((rows + tg::kPxRows - 1) / tg::kPxRows), (unsigned)((G.N0 + tg::kPxCols - 1) / tg::kPxCols));
+    tg::k_prolong_x<T, T><<<gx, tg::kPxThreads, 0, c->stream>>>(rows, G.N0, c->Nc[0], c->tA, c->tPt[0], r, s, out);
+    CKL();
+  }
 }
 
 // Coarse Jacobian of the current Newton step: c'_H = R d, d = c'(t) fine.
@@ -1691,6 +1747,22 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
           c->tRt[a] = up(Rt);
           c->tP[a] = up(P);
           c->tPt[a] = up(Pt);
+        }
+        {  // x-axis FFT-transfer tables, K = Nc0 / 2: C [K+1][Nc0], D [Nc0][K+1]
+          const int ncx = c->Nc[0], K = ncx / 2, n0 = pd->N[0];
+          std::vector<float2> Ct((size_t)(K + 1) * ncx), Dt((size_t)(K + 1) * ncx);
+          for (int k = 0; k <= K; ++k)
+            for (int i = 0; i < ncx; ++i) {
+              const double ph = 2.0 * pi * ((long long)k * i % ncx) / ncx;
+              const double ck = (k == 0 || 2 * k == ncx) ? 1.0 : 2.0;
+              const double fk = (2 * k == ncx) ? 0.5 / ncx : 1.0 / ncx;
+              Ct[(size_t)k * ncx + i] = make_float2((float)(ck * std::cos(ph) / n0), (float)(ck * std::sin(ph) / n0));
+              Dt[(size_t)i * (K + 1) + k] = make_float2((float)(fk * std::cos(ph)), (float)(-fk * std::sin(ph)));
+            }
+          c->tC = dalloc<float2>(Ct.size());
+          c->tD = dalloc<float2>(Dt.size());
+          CK(cudaMemcpy(c->tC, Ct.data(), sizeof(float2) * Ct.size(), cudaMemcpyHostToDevice));
+          CK(cudaMemcpy(c->tD, Dt.data(), sizeof(float2) * Dt.size(), cudaMemcpyHostToDevice));
         }
         c->tA = dalloc<float>((size_t)m * G.N2 * G.N1 * c->Nc[0]);
         c->tB = dalloc<float>((size_t)m * G.N2 * c->Nc[1] * c->Nc[0]);

@@ -1,0 +1,215 @@
+// twogrid_fft.cuh -- the x-axis grid transfers of the two-grid
+// preconditioner by FFT, for the row lengths with shape-specialised
+// transforms (N0 = 2M).
+//
+// Restriction of a row x (N0 reals) to Nc coarse points, K = Nc/2:
+//   out_i = (s/N0) [X_0 + 2 sum_{0<k<K} Re(e^{2 pi i k i/Nc} X_k) + Re(e^{2 pi i K i/Nc} X_K)],
+// X = r2c(x) -- only X_0..X_K are formed after the row transform.
+// Prolongation of a coarse row y (Nc reals) with the residual term:
+//   out_j = c2r(X)_j - s r_j,  X_k = f_k sum_i y_i e^{-2 pi i k i/Nc},
+// f_k = 1/Nc for k < K, 1/(2 Nc) at the Nyquist k = K, X_k = 0 above K.
+// Both equal the dense band-limited transfers of twogrid.cuh (the same
+// R and P) at about a third of the arithmetic: the row transform is the
+// half-length complex FFT of the x passes plus the r2c untangle, and the
+// coarse side is a (K+1) x Nc table product.  Transforms run in FP32.
+#pragma once
+#include "fft_static.cuh"
+
+namespace rism {
+
+template <typename T> __device__ __forceinline__ float2 ld_pair(const T *p);
+template <> __device__ __forceinline__ float2 ld_pair<float>(const float *p) {
+  return *reinterpret_cast<const float2 *>(p);
+}
+template <> __device__ __forceinline__ float2 ld_pair<double>(const double *p) {
+  const double2 v = *reinterpret_cast<const double2 *>(p);
+  return make_float2((float)v.x, (float)v.y);
+}
+
+template <int M, int RX> __host__ __device__ constexpr int fx_buf() { return RX * LayRow<M, Split<M>::R2>::RS; }
+
+// Shared memory of the two kernels (bytes) for K = Nc/2: twiddles, the row
+// tiles, the coarse-side table, the kept spectrum (and the coarse rows).
+template <int M, int RX> inline size_t fx_smem_restrict(int K, int Nc) {
+  return sizeof(float2) * (size_t)(M + fx_buf<M, RX>() + (K + 1) * Nc + RX * (K + 1));
+}
+template <int M, int RX> inline size_t fx_smem_prolong(int K, int Nc) {
+  return sizeof(float2) * (size_t)(M + fx_buf<M, RX>() + (K + 1) * Nc + RX * (K + 1)) +
+         sizeof(float) * (size_t)RX * Nc;
+}
+
+// Vector access of 2 complex values (4 reals) of a row.
+template <typename T> struct Quad;
+template <> struct Quad<float> {
+  using type = float4;
+  __device__ __forceinline__ static void split(const float4 &v, float2 &a, float2 &b) {
+    a = make_float2(v.x, v.y);
+    b = make_float2(v.z, v.w);
+  }
+};
+template <> struct Quad<double> {
+  struct type { double2 a, b; };
+  __device__ __forceinline__ static void split(const type &v, float2 &a, float2 &b) {
+    a = make_float2((float)v.a.x, (float)v.a.y);
+    b = make_float2((float)v.b.x, (float)v.b.y);
+  }
+};
+
+// out[row][i] (rows x Nc, FP32) = restriction of s * in[row][.] (rows x 2M).
+// ctab[k][i] = c_k e^{2 pi i k i / Nc} / N0, c = 1, 2, ..., 2, 1.
+template <typename TI, int M, int RX>
+__global__ void __launch_bounds__(256) k_restrict_fx(long long rows, int Nc, int K, const TI *__restrict__ in,
+                                                     float s, const float2 *__restrict__ post,
+                                                     const float2 *__restrict__ twg,
+                                                     const float2 *__restrict__ ctab, float *__restrict__ out) {
+  using V = float2;
+  using Lay = LayRow<M, Split<M>::R2>;
+  using Q = typename Quad<TI>::type;
+  constexpr int N0 = 2 * M, PER = M / 2, CNT = (RX * PER + 255) / 256;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V *tw = reinterpret_cast<V *>(smem_raw);
+  V *buf = tw + M;
+  V *C = buf + fx_buf<M, RX>();
+  const int K1 = K + 1;
+  V *X = C + K1 * Nc;
+  const int tid = threadIdx.x;
+  const long long row0 = (long long)blockIdx.x * RX;
+  // all row loads in flight before any use
+  Q ra[CNT];
+#pragma unroll
+  for (int it = 0; it < CNT; ++it) {
+    const int e = tid + it * 256;
+    const int row = e / PER, jj = (e % PER) * 2;
+    if (e < RX * PER && row0 + row < rows) ra[it] = *reinterpret_cast<const Q *>(in + (row0 + row) * N0 + 2 * jj);
+  }
+  for (int q = tid; q < M; q += 256) tw[q] = twg[q];
+  for (int q = tid; q < K1 * Nc; q += 256) C[q] = ctab[q];
+#pragma unroll
+  for (int it = 0; it < CNT; ++it) {
+    const int e = tid + it * 256;
+    if (e >= RX * PER) break;
+    const int row = e / PER, jj = (e % PER) * 2;
+    V a = make_float2(0.f, 0.f), b = a;
+    if (row0 + row < rows) {
+      Quad<TI>::split(ra[it], a, b);
+      a.x *= s; a.y *= s; b.x *= s; b.y *= s;
+    }
+    buf[Lay::at(jj, row)] = a;
+    buf[Lay::at(jj + 1, row)] = b;
+  }
+  __syncthreads();
+  fft2<M, RX, 256, false, false, Lay>(buf, tw);
+  for (int e = tid; e < RX * K1; e += 256) {
+    const int row = e / K1, k = e - row * K1;
+    const V zk = buf[Lay::at(k, row)];
+    const V zm = buf[Lay::at(k == 0 ? 0 : M - k, row)];
+    V E, O;
+    E.x = (zk.x + zm.x) * 0.5f;
+    E.y = (zk.y - zm.y) * 0.5f;
+    O.x = (zk.y + zm.y) * 0.5f;
+    O.y = -(zk.x - zm.x) * 0.5f;
+    X[row * K1 + k] = cadd(E, cmul(post[k], O));
+  }
+  __syncthreads();
+  for (int e = tid; e < RX * Nc; e += 256) {
+    const int row = e / Nc, i = e - row * Nc;
+    if (row0 + row >= rows) continue;
+    float acc = 0.f;
+    for (int k = 0; k < K1; ++k) {
+      const V c = C[k * Nc + i], x = X[row * K1 + k];
+      acc = fmaf(c.x, x.x, fmaf(-c.y, x.y, acc));
+    }
+    out[(row0 + row) * Nc + i] = acc;
+  }
+}
+
+// out[row][j] (rows x 2M) = prolongation of y[row][.] (rows x Nc, FP32) - s r.
+// dtab[i][k] = f_k e^{-2 pi i k i / Nc} (k fastest).
+template <typename TO, typename TR, int M, int RX>
+__global__ void __launch_bounds__(256) k_prolong_fx(long long rows, int Nc, int K, const float *__restrict__ y,
+                                                    const float2 *__restrict__ post, const float2 *__restrict__ twg,
+                                                    const float2 *__restrict__ dtab, const TR *__restrict__ r,
+                                                    double s, TO *__restrict__ out) {
+  using V = float2;
+  using Lay = LayRow<M, Split<M>::R2>;
+  using QR = typename Quad<TR>::type;
+  constexpr int N0 = 2 * M, H = M / 2 + 1, PER = M / 2, CNT = (RX * PER + 255) / 256;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V *tw = reinterpret_cast<V *>(smem_raw);
+  V *buf = tw + M;
+  const int K1 = K + 1;
+  V *D = buf + fx_buf<M, RX>();
+  V *X = D + K1 * Nc;
+  float *ys = reinterpret_cast<float *>(X + RX * K1);
+  const int tid = threadIdx.x;
+  const long long row0 = (long long)blockIdx.x * RX;
+  // the subtracted rows are fetched first; their latency hides behind the work
+  QR rr[CNT];
+#pragma unroll
+  for (int it = 0; it < CNT; ++it) {
+    const int e = tid + it * 256;
+    const int row = e / PER, jj = (e % PER) * 2;
+    if (e < RX * PER && row0 + row < rows) rr[it] = *reinterpret_cast<const QR *>(r + (row0 + row) * N0 + 2 * jj);
+  }
+  for (int q = tid; q < M; q += 256) tw[q] = twg[q];
+  for (int q = tid; q < K1 * Nc; q += 256) D[q] = dtab[q];
+  for (int e = tid; e < RX * Nc; e += 256) ys[e] = (row0 + e / Nc < rows) ? y[row0 * Nc + e] : 0.f;
+  __syncthreads();
+  for (int e = tid; e < RX * K1; e += 256) {
+    const int row = e / K1, k = e - row * K1;
+    float ax = 0.f, ay = 0.f;
+    for (int i = 0; i < Nc; ++i) {
+      const V d = D[i * K1 + k];
+      const float v = ys[row * Nc + i];
+      ax = fmaf(d.x, v, ax);
+      ay = fmaf(d.y, v, ay);
+    }
+    X[row * K1 + k] = make_float2(ax, ay);
+  }
+  __syncthreads();
+  for (int e = tid; e < RX * H; e += 256) {
+    const int row = e / H, k = e - row * H;
+    V xk = make_float2(0.f, 0.f), xm = make_float2(0.f, 0.f);
+    if (k <= K) xk = X[row * K1 + k];
+    if (M - k <= K) xm = X[row * K1 + (M - k)];
+    if (k == 0) { xk.y = 0.f; xm.y = 0.f; }
+    V Aa, Dd;
+    Aa.x = xk.x + xm.x; Aa.y = xk.y - xm.y;
+    Dd.x = xk.x - xm.x; Dd.y = xk.y + xm.y;
+    const V Pp = cmul(Dd, cconj(post[k]));
+    V zk, zm;
+    zk.x = Aa.x - Pp.y; zk.y = Aa.y + Pp.x;
+    zm.x = Aa.x + Pp.y; zm.y = -(Aa.y - Pp.x);
+    buf[Lay::at(k, row)] = zk;
+    if (k != 0 && M - k != k) buf[Lay::at(M - k, row)] = zm;
+  }
+  __syncthreads();
+  fft2<M, RX, 256, true, false, Lay>(buf, tw);
+#pragma unroll
+  for (int it = 0; it < CNT; ++it) {
+    const int e = tid + it * 256;
+    if (e >= RX * PER) break;
+    const int row = e / PER, jj = (e % PER) * 2;
+    if (row0 + row >= rows) continue;
+    V ra, rb;
+    Quad<TR>::split(rr[it], ra, rb);
+    const V za = buf[Lay::at(jj, row)], zb = buf[Lay::at(jj + 1, row)];
+    TO *o = out + (row0 + row) * N0 + 2 * jj;
+    // the subtracted term in the output precision (r kept exact for FP64)
+    const TR *rx = r + (row0 + row) * N0 + 2 * jj;
+    if (sizeof(TR) == 8) {
+      o[0] = (TO)((double)za.x - s * (double)rx[0]);
+      o[1] = (TO)((double)za.y - s * (double)rx[1]);
+      o[2] = (TO)((double)zb.x - s * (double)rx[2]);
+      o[3] = (TO)((double)zb.y - s * (double)rx[3]);
+    } else {
+      const float sf = (float)s;
+      o[0] = (TO)(za.x - sf * ra.x);
+      o[1] = (TO)(za.y - sf * ra.y);
+      o[2] = (TO)(zb.x - sf * rb.x);
+      o[3] = (TO)(zb.y - sf * rb.y);
+    }
+  }
+}
+
+}  // namespace rism

@@ -121,6 +121,35 @@ def test_preconditioner_matches_numpy(fixture_loader, name, graph, monkeypatch):
     ctx.close()
 
 
+@pytest.mark.parametrize("n, L", [(64, 9.0), (128, 24.0)])
+def test_fft_transfers_match_dense(fixture_loader, n, L):
+    """At row lengths with shape-specialised transforms the x-axis transfers
+    run by FFT; the preconditioner still equals the dense restatement."""
+    meta, arr = fixture_loader("synth6_kh_n32")
+    steps = 12
+    s = settings_of(meta, N=n, L=L, **{"coarse-steps": steps})
+    ctx = RismContext(meta["solute"], meta["solvent"], s, arr["chi"])
+    nc = ctx.coarse_grid()
+    assert nc is not None and nc[0] < n
+    R, Pm = transfer(n, nc[0])
+    Pc = problem(meta, arr["chi"], nc[0], L=L)
+    P = problem(meta, arr["chi"], n, L=L)
+    rng = np.random.default_rng(8)
+    T = 0.3 * rng.standard_normal(ctx.shape)
+    v = rng.standard_normal(ctx.shape)
+    z = ctx.precondition(to_dev(T), to_dev(v)).cpu().numpy()
+    d = cl.closure1(int(meta["settings"]["closure"]), meta["settings"]["beta"], P.v, T, np.ones_like(T))
+    dH = along(R, d)
+
+    def JH(u):
+        return Pc.ifft(Pc.star(Pc.fft(dH * u) * Pc.h3)) * (1.0 / Pc.L3) - u
+
+    rc = along(R, v)
+    z_ref = along(Pm, gmres_steps(JH, rc, steps) + rc) - v
+    assert np.max(np.abs(z - z_ref)) < 1e-4 * np.max(np.abs(z_ref))
+    ctx.close()
+
+
 @pytest.mark.parametrize("name", ["water_hnc_n24", "synth6_kh_n32", "synth6_pse3_n32"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_preconditioned_solve_reaches_the_root(fixture_loader, name, precision):
