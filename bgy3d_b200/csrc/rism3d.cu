@@ -1701,16 +1701,28 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
       OPTIN_S(float)
 #undef OPTIN_S
     }
-    // two-grid preconditioner: a copy of the problem on a grid of about
-    // coarse_h spacing, used when that grid is coarser along every axis
+    // two-grid preconditioner: a copy of the problem on a coarse grid.  The
+    // spacing coarse_h is taken when its grid has at most half the fine
+    // points along every axis (a coarse solve costs ~12 coarse J.v per fine
+    // iteration); otherwise 1 A (or coarse_h if coarser), when that grid is
+    // still coarser than the fine one; otherwise the preconditioner is off.
     if (pd->coarse_h > 0 && pd->solver != RISM3D_PICARD) {
+      auto grid_for = [&](double h, int *nc) {
+        bool half = true;
+        for (int a = 0; a < 3; ++a) {
+          int nn = std::max(8, (int)std::ceil(pd->L[a] / h - 1e-9));
+          while (!(is_2a3b(nn) && nn % 2 == 0)) ++nn;
+          nc[a] = nn;
+          if (2 * nn > pd->N[a]) half = false;
+        }
+        return half;
+      };
       int nc[3];
       bool coarser = true;
-      for (int a = 0; a < 3; ++a) {
-        int nn = std::max(8, (int)std::ceil(pd->L[a] / pd->coarse_h - 1e-9));
-        while (!(is_2a3b(nn) && nn % 2 == 0)) ++nn;
-        nc[a] = nn;
-        if (nn >= pd->N[a]) coarser = false;
+      if (!grid_for(pd->coarse_h, nc)) {
+        grid_for(std::max(pd->coarse_h, 1.0), nc);
+        for (int a = 0; a < 3; ++a)
+          if (nc[a] >= pd->N[a]) coarser = false;
       }
       if (coarser) {
         rism3d_problem pc = *pd;
@@ -1817,7 +1829,7 @@ void rism3d_problem_defaults(rism3d_problem *pd, double L_half, int N) {
   pd->verbosity = 0;
   pd->krylov_restart = 30;
   pd->ew_forcing = 1;
-  pd->coarse_h = 1.0;
+  pd->coarse_h = 0.75;
   pd->coarse_steps = 12;
 }
 

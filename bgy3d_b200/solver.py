@@ -28,7 +28,7 @@ DEFAULTS = {
     # forcing (0: the reference's fixed rtol 1e-3), the two-grid
     # preconditioner's coarse spacing in A (0: off, the reference's
     # unpreconditioned GMRES) and its coarse GMRES steps.
-    "krylov-restart": 30, "ew-forcing": 1, "coarse-h": 1.0, "coarse-steps": 12,
+    "krylov-restart": 30, "ew-forcing": 1, "coarse-h": 0.75, "coarse-steps": 12,
 }
 
 

@@ -86,15 +86,16 @@ typedef struct rism3d_problem {
   /* Krylov solver of the Newton steps.  krylov_restart 30, ew_forcing 0 and
      coarse_h 0 are the reference's settings: GMRES(30) without
      preconditioner at a fixed KSP rtol of 1e-3 (bgy3d-snes.c:262-306).
-     rism3d_problem_defaults() selects 30 / 1 / 1.0 / 12. */
+     rism3d_problem_defaults() selects 30 / 1 / 0.75 / 12. */
   int krylov_restart; /* GMRES restart length (0: 30) */
   int ew_forcing;     /* 1: Eisenstat-Walker forcing terms, floored at 1e-3;
                          0: fixed rtol 1e-3 */
   double coarse_h;    /* two-grid preconditioner (then flexible GMRES):
                          coarse grid spacing in A -- per axis the smallest
-                         even 2^a 3^b point count n with L / n <= coarse_h;
-                         off when 0 or when that grid is not coarser than N
-                         along every axis */
+                         even 2^a 3^b point count n with L / n <= coarse_h,
+                         used when n <= N/2 on every axis; otherwise the
+                         grid of max(coarse_h, 1 A) spacing if it is coarser
+                         than N on every axis; off when 0 or neither fits */
   int coarse_steps;   /* GMRES steps of each coarse solve (0: 12) */
 } rism3d_problem;
 
