@@ -196,6 +196,7 @@ struct rism3d_ctx {
   float2 *chi32 = nullptr, *s32 = nullptr;
   void *W = nullptr;  // complex work buffer, FP64-sized, reused by the FP32 path
   SiteP *d_solute = nullptr, *d_solvent = nullptr;
+  int n_cap = 0;  // capacity of d_solute
   double *d_charge = nullptr;
 
   NormPartial *npart = nullptr;
@@ -1416,6 +1417,40 @@ int gradient_impl(rism3d_ctx *c, const double *T, rism3d_grad *gr) {
   return RISM3D_OK;
 }
 
+// (Re)binds the solute: its device copy, the short-range field v (FP64 and
+// FP32) and the long-range field L; grid, chi tables and work buffers stay.
+void bind_solute(rism3d_ctx *c, int n, const rism3d_site *solute) {
+  const Geo &G = c->g;
+  const rism3d_problem &pd = c->pd;
+  std::vector<SiteP> hs(std::max(n, 1));
+  for (int u = 0; u < n; ++u)
+    hs[u] = SiteP{solute[u].x[0], solute[u].x[1], solute[u].x[2], solute[u].sigma, solute[u].epsilon,
+                  solute[u].charge};
+  if (!c->d_solute || n > c->n_cap) {
+    dfree(c->d_solute);
+    c->n_cap = std::max(n, 1);
+    c->d_solute = dalloc<SiteP>(c->n_cap);
+  }
+  CK(cudaMemcpyAsync(c->d_solute, hs.data(), sizeof(SiteP) * std::max(n, 1), cudaMemcpyHostToDevice, c->stream));
+  c->n = n;
+  c->solute.assign(solute, solute + n);
+  const double h0 = pd.L[0] / pd.N[0], h1 = pd.L[1] / pd.N[1], h2 = pd.L[2] / pd.N[2];
+  const unsigned nb = (unsigned)((G.Nr + 255) / 256);
+  k_field0<<<nb, 256, 0, c->stream>>>(G, h0, h1, h2, pd.L[0], pd.L[1], pd.L[2], c->d_solvent, n, c->d_solute,
+                                      c->v64);
+  CKL();
+  k_axpby<double, float><<<vec_grid(c->nvec), 256, 0, c->stream>>>(c->nvec, 1.0, c->v64, 0.0, c->v32);
+  CKL();
+  CK(cudaMemsetAsync(c->L64, 0, sizeof(double2) * (size_t)G.Nhp * G.N1 * G.N2, c->stream));
+  CK(cudaMemsetAsync(c->L32, 0, sizeof(float2) * (size_t)G.Nhp * G.N1 * G.N2, c->stream));
+  const long long nk = (long long)G.Nh * G.N1 * G.N2;
+  k_longrange<<<(unsigned)((nk + 255) / 256), 256, 0, c->stream>>>(G, n, c->d_solute, pd.renorm, 1.0 / c->h3,
+                                                                   c->L64, c->L32);
+  CKL();
+  CK(cudaStreamSynchronize(c->stream));  // hs is freed on return
+  if (c->coarse) bind_solute(c->coarse, n, solute);
+}
+
 int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int n, const rism3d_site *solute,
                 const double *chi, rism3d_ctx **out) {
   if (!pd || !solvent || (!solute && n > 0) || !chi || !out) throw ArgFail{RISM3D_ERR_ARG, "null argument"};
@@ -1542,37 +1577,22 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
     CK(cudaMemcpy(c->s32, s32.data(), sizeof(float2) * s32.size(), cudaMemcpyHostToDevice));
 
     // sites
-    std::vector<SiteP> hs(std::max(n, 1)), hv(m);
-    for (int u = 0; u < n; ++u)
-      hs[u] = SiteP{solute[u].x[0], solute[u].x[1], solute[u].x[2], solute[u].sigma, solute[u].epsilon,
-                    solute[u].charge};
+    std::vector<SiteP> hv(m);
     for (int i = 0; i < m; ++i)
       hv[i] = SiteP{solvent[i].x[0], solvent[i].x[1], solvent[i].x[2], solvent[i].sigma, solvent[i].epsilon,
                     solvent[i].charge};
-    c->d_solute = dalloc<SiteP>(std::max(n, 1));
-    CK(cudaMemcpy(c->d_solute, hs.data(), sizeof(SiteP) * std::max(n, 1), cudaMemcpyHostToDevice));
-    SiteP *d_solvent = c->d_solvent = dalloc<SiteP>(m);
-    CK(cudaMemcpy(d_solvent, hv.data(), sizeof(SiteP) * m, cudaMemcpyHostToDevice));
+    c->d_solvent = dalloc<SiteP>(m);
+    CK(cudaMemcpy(c->d_solvent, hv.data(), sizeof(SiteP) * m, cudaMemcpyHostToDevice));
     c->d_charge = dalloc<double>(m);
     CK(cudaMemcpy(c->d_charge, c->charge.data(), sizeof(double) * m, cudaMemcpyHostToDevice));
 
-    // fields
+    // fields of the solute
     c->v64 = dalloc<double>(c->nvec);
     c->v32 = dalloc<float>(c->nvec);
-    const unsigned nb = (unsigned)((G.Nr + 255) / 256);
-    k_field0<<<nb, 256>>>(G, h0, h1, h2, pd->L[0], pd->L[1], pd->L[2], d_solvent, n, c->d_solute, c->v64);
-    CKL();
-    k_axpby<double, float><<<vec_grid(c->nvec), 256>>>(c->nvec, 1.0, c->v64, 0.0, c->v32);
-    CKL();
     c->L64 = dalloc<double2>((size_t)G.Nc);
     c->L32 = dalloc<float2>((size_t)G.Nc);
-    CK(cudaMemset(c->L64, 0, sizeof(double2) * (size_t)G.Nhp * G.N1 * G.N2));
-    CK(cudaMemset(c->L32, 0, sizeof(float2) * (size_t)G.Nhp * G.N1 * G.N2));
-    const long long nk = (long long)G.Nh * G.N1 * G.N2;
-    k_longrange<<<(unsigned)((nk + 255) / 256), 256>>>(G, n, c->d_solute, pd->renorm, 1.0 / c->h3, c->L64,
-                                                       c->L32);
-    CKL();
-    CK(cudaStreamSynchronize(cudaStreamPerThread));
+    bind_solute(c, n, solute);
+    (void)h0; (void)h1; (void)h2;
     c->W = dalloc<double2>((size_t)m * G.Nc);
     // reduction blocks: about four 16-byte loads per thread, at most 4 per SM
     c->red_blocks = (int)std::min<long long>(592, std::max<long long>(8, (c->nvec / 4 + 1023) / 1024));
@@ -1982,6 +2002,14 @@ int rism3d_solve_batch(int m, const rism3d_site *solvent, int njobs, rism3d_job 
   int rc = RISM3D_OK;
   for (int i = 0; i < njobs && rc == RISM3D_OK; ++i) rc = jobs[i].result.status;
   return rc;
+}
+
+int rism3d_ctx_set_solute(rism3d_ctx *ctx, int n, const rism3d_site *solute) {
+  if (!ctx || n < 0 || (n > 0 && !solute)) return RISM3D_ERR_ARG;
+  return guard([&] {
+    bind_solute(ctx, n, solute);
+    return (int)RISM3D_OK;
+  });
 }
 
 int rism3d_jacobian_transpose_t1(rism3d_ctx *ctx, const double *T, const double *dT, double *JT) {

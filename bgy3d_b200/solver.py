@@ -301,6 +301,13 @@ class RismContext:
                       self._check_vec(out, T.dtype)), "jacobian_t1")
         return out
 
+    def set_solute(self, solute):
+        """Rebind to another solute (geometry, charges, LJ) of the same
+        solvent and grid without setting the context up again; a following
+        solve(T) may start from the previous T (rism3d_ctx_set_solute)."""
+        _abi.check(_abi.lib().rism3d_ctx_set_solute(self._h, len(solute), _sites(solute)), "set_solute")
+        self.n = len(solute)
+
     def coarse_grid(self):
         """Points per axis of the two-grid preconditioner's coarse grid
         (None when it is off)."""

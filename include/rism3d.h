@@ -258,6 +258,15 @@ const char *rism3d_last_error(void);
    RISM3D_ERR_UNSUPPORTED when the context has no coarse grid. */
 int rism3d_precondition(rism3d_ctx *ctx, const double *T, const double *v, double *z);
 
+/* Rebinds the context to another solute of the same solvent and grid (a
+   new geometry, charges or LJ parameters): recomputes the solute's
+   short-range field and long-range term only, keeping every buffer, the
+   chi tables and the preconditioner's coarse problem, so that consecutive
+   solves of a PES scan or a geometry optimisation (the restart loop of
+   guile/bgy3d.scm:819-880 with hnc3d.c:1830-1845) pay no setup and can
+   start from the previous t.  n may differ from the creating call's. */
+int rism3d_ctx_set_solute(rism3d_ctx *ctx, int n, const rism3d_site *solute);
+
 /* The transposed Jacobian at T (the adjoint operator of the gradient):
    JT = J^T dT = c'(T) . ((chi - 1) * dT) - dT.  FP64 device pointers. */
 int rism3d_jacobian_transpose_t1(rism3d_ctx *ctx, const double *T, const double *dT, double *JT);
