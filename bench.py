@@ -25,7 +25,8 @@ Beside the timed line (unless --no-extras): "batch", 64 solutes of 3-40
 sites on grids 64^3..192^3 solved by rism3d_solve_batch in mixed and FP64
 precision (aggregate solves/s, per-solute |dmu|); "gradient", the adjoint
 dmu/d(q, sigma, eps, x) of the workload's solute (time against one
-solve, central-difference checks).
+solve, central-difference checks); "pes", an 8-point scan of the solute
+rebound on one context with warm starts, against fresh solves.
 
   python bench.py --profile-solve   one warm mixed solve between
                                     cudaProfilerStart/Stop (for ncu
@@ -152,6 +153,44 @@ def run_gradient_report(solute, solvent, s, chi, ms_solve):
             "gradient_over_solve": g["seconds"] / (ms_solve * 1e-3), "adjoint_jv": g["adjoint-jv"],
             "adjoint_resid": g["adjoint-resid"], "fd_checks": checks,
             "params": "dmu/d{q, sigma, eps, x} of all %d sites" % len(solute)}
+
+
+def run_pes_report(solute, solvent, s, chi, points=8, step=0.05):
+    """A PES scan of the workload's solute (site 0 moved along x in steps of
+    0.05 A): one context rebound per point with the solve warm-started from
+    the previous t, against a fresh rism3d_solute_solve per point."""
+    import torch
+    from bgy3d_b200 import RismContext, hnc3d_run_solute
+    st = dict(s, precision="mixed")
+
+    def moved(k):
+        out = [dict(a) for a in solute]
+        x = list(out[0]["x"])
+        x[0] += step * k
+        out[0]["x"] = tuple(x)
+        return out
+
+    geoms = [moved(k) for k in range(points)]
+    ctx = RismContext(solute, solvent, st, chi)
+    T, _ = ctx.solve()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    iters = []
+    for g in geoms:
+        ctx.set_solute(g)
+        T, r = ctx.solve(T)
+        iters.append(r["newton-iters"])
+    torch.cuda.synchronize()
+    warm = time.perf_counter() - t0
+    ctx.close()
+    t0 = time.perf_counter()
+    for g in geoms:
+        hnc3d_run_solute(g, solvent, st, chi, want_g=False, want_restart=False)
+    torch.cuda.synchronize()
+    fresh = time.perf_counter() - t0
+    return {"points": points, "step_A": step, "rebind_warm_solves_per_s": points / warm,
+            "fresh_solves_per_s": points / fresh, "newton_per_point": iters,
+            "timing": "host clock around the scan"}
 
 
 def config(grid=GRID, precision="mixed"):
@@ -354,6 +393,7 @@ def run_ours(args, rank, world):
     if world == 1 and not args.no_extras:
         line["batch"] = run_batch_report(solvent, s, chi)
         line["gradient"] = run_gradient_report(solute, solvent, s, chi, ms / args.steps)
+        line["pes"] = run_pes_report(solute, solvent, s, chi)
     return line
 
 
