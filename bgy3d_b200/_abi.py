@@ -76,6 +76,7 @@ EXPORTS = [
     "rism3d_profile", "rism1d_solvent_chi", "rism3d_jacobian_apply_noalloc",
     "rism3d_precondition", "rism3d_coarse_grid", "rism3d_solve_batch",
     "rism3d_solute_grad", "rism3d_gradient", "rism3d_jacobian_transpose_t1", "rism3d_ctx_set_solute",
+    "rism3d_response",
 ]
 
 _lib = None
@@ -134,6 +135,8 @@ def lib():
     L.rism3d_jacobian_transpose_t1.restype = I
     L.rism3d_ctx_set_solute.argtypes = [V, I, P(Site)]
     L.rism3d_ctx_set_solute.restype = I
+    L.rism3d_response.argtypes = [V, V, P(Grad)]
+    L.rism3d_response.restype = I
     _lib = L
     return L
 

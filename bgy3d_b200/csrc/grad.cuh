@@ -232,4 +232,97 @@ static __global__ void k_dmul_sub(long long n, const double *__restrict__ d, con
     out[i] = d[i] * a[i] - b[i];
 }
 
+
+// ---------------------------------------------------------- linear response
+// dmu/dR by forward-mode linear response (the response branch of
+// hnc3d_solute_solve, hnc3d.c:1969-2135, with response_t1, 1366-1421): per
+// unit displacement of one solute site, dv = field1 (LJ plus the FULL capped
+// Coulomb, bgy3d-solutes.c:381-468), J dT = beta K ((c' + 1) dv), and the
+// differential of the free-energy density form1 (closures.f90:615-653).
+
+// d ccap0 / dr, the capped full Coulomb 1/r (bgy3d-solutes.c:275-283): -1/r^2
+// beyond R, the capped short-range plus long-range parts inside.
+__device__ __forceinline__ double ccap1(double r) {
+  const double R = 0.2;
+  if (r >= R) return -1.0 / (r * r);
+  return r * (cs1(R) / R + cl1s(r));
+}
+
+// Differential of form(method, x, h, c, cl) (closures.f90:615-653).
+__device__ __forceinline__ double form1(int method, double x, double dx, double h, double dh, double c, double dc,
+                                        double cl) {
+  const double base = -dc - dh * (c + cl) / 2 - h * dc / 2;
+  switch (method) {
+    case CL_HNC: return base + h * dh;
+    case CL_KH: return h < 0 ? base + h * dh : base;
+    case CL_PY: return base;
+    default: {
+      if (h < 0) return base + h * dh;
+      const int n = method - CL_PSE0;
+      double xn = 1.0;
+      for (int k = 0; k < n; ++k) xn *= x;
+      return base + (h * dh - xn * dx / dfact(n));
+    }
+  }
+}
+
+// dv[s] = d v_s / d R_{u,dim} on the grid (field1 for one moving site).
+static __global__ void k_field1(Geo g, double h0, double h1, double h2, double L0, double L1, double L2,
+                                const SiteP *__restrict__ solvent, const SiteP *__restrict__ solute, int u, int dim,
+                                double *__restrict__ dv) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= g.Nr) return;
+  const int i0 = (int)(p % g.N0);
+  const int i1 = (int)((p / g.N0) % g.N1);
+  const int i2 = (int)(p / ((long long)g.N0 * g.N1));
+  const SiteP b = solute[u];
+  const double ab[3] = {i0 * h0 - L0 / 2 - b.x, i1 * h1 - L1 / 2 - b.y, i2 * h2 - L2 / 2 - b.z};
+  const double r = sqrt(ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2]);
+  const double dr = r > 0.0 ? -ab[dim] / r : 0.0;
+  for (int s = 0; s < g.m; ++s) {
+    const SiteP a = solvent[s];
+    const double eab = sqrt(a.epsilon * b.epsilon), sab = 0.5 * (a.sigma + b.sigma);
+    const double qab = a.charge * b.charge * kEps0Inv;
+    dv[(long long)s * g.Nr + p] = dr * ((eab / sab) * ljcap1(r / sab) + qab * kG * kG * ccap1(kG * r));
+  }
+}
+
+// out = d + 1 (the closure's dh/dx, the slope the flagged Jacobian applies).
+static __global__ void k_shift1(long long n, const double *__restrict__ d, double *__restrict__ out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = d[i] + 1.0;
+}
+
+// Block partials of sum_r sum_s form1(x, dx, h, dh, c, dc, cl) with
+// dx = -beta dv + dT, dc = c' dx - beta dv, dh = dc + dT (hnc3d.c:2063-2097).
+static __global__ void __launch_bounds__(256) k_mu1(Geo g, const double *__restrict__ t,
+                                                    const double *__restrict__ v, const double *__restrict__ uc,
+                                                    const double *__restrict__ dv, const double *__restrict__ dT,
+                                                    double beta, int closure, const double *__restrict__ charge,
+                                                    double *__restrict__ part) {
+  double acc = 0.0;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.Nr;
+       p += (long long)gridDim.x * blockDim.x) {
+    for (int s = 0; s < g.m; ++s) {
+      const long long o = (long long)s * g.Nr + p;
+      const double ts = t[o], bv = beta * v[o];
+      const double c = closure_c<double>(closure, bv, ts), d = closure_d<double>(closure, bv, ts);
+      const double h = c + ts, x = -bv + ts, cl = -beta * charge[s] * uc[p];
+      const double bdv = beta * dv[o], dt = dT[o];
+      const double dx = -bdv + dt, dc = d * dx - bdv, dh = dc + dt;
+      acc += form1(closure, x, dx, h, dh, c, dc, cl);
+    }
+  }
+  __shared__ double sm[8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) sm[wid] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a += sm[w];
+    part[blockIdx.x] = a;
+  }
+}
+
 }  // namespace rism

@@ -1417,6 +1417,84 @@ int gradient_impl(rism3d_ctx *c, const double *T, rism3d_grad *gr) {
   return RISM3D_OK;
 }
 
+// Linear-response dmu/dR (the response branch of hnc3d_solute_solve): one
+// preconditioned FGMRES solve J dT = beta K((c' + 1) dv) per unit
+// displacement, then the free-energy differential reduced on the device.
+int response_impl(rism3d_ctx *c, const double *T, rism3d_grad *gr) {
+  const rism3d_problem &pd = c->pd;
+  if (pd.closure == 2) {
+    g_last_error = "PY has no closure differential";
+    return RISM3D_ERR_UNSUPPORTED;
+  }
+  const Geo &G = c->g;
+  const long long nv = c->nvec;
+  const double h0 = pd.L[0] / pd.N[0], h1 = pd.L[1] / pd.N[1], h2 = pd.L[2] / pd.N[2];
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, c->stream));
+  const unsigned nb = (unsigned)((G.Nr + 255) / 256);
+  double *uc = dalloc<double>(G.Nr);
+  k_coulomb_long<<<nb, 256, 0, c->stream>>>(G, h0, h1, h2, pd.L[0], pd.L[1], pd.L[2], c->n, c->d_solute, uc);
+  CKL();
+  double *d = slopebuf<double>(c);
+  closure_slope<double, double>(c, T, d);
+  double *d1 = dalloc<double>(nv), *dv = dalloc<double>(nv), *B = dalloc<double>(nv), *dT = dalloc<double>(nv);
+  double *Bc = dalloc<double>(nv);
+  k_shift1<<<vec_grid(nv), 256, 0, c->stream>>>(nv, d, d1);
+  CKL();
+  const int restart = pd.krylov_restart > 0 ? std::min(pd.krylov_restart, 200) : 30;
+  if (c->coarse) tg_prepare<double>(c, d);
+  const int n = c->n;
+  const int rb = (int)std::min<long long>(2 * 148, (G.Nr + 255) / 256);
+  double *part = dalloc<double>((size_t)rb * 3 * std::max(n, 1));
+  const int jv0 = c->jv_evals;
+  double worst = 0.0;
+  for (int u = 0; u < n; ++u)
+    for (int dim = 0; dim < 3; ++dim) {
+      k_field1<<<nb, 256, 0, c->stream>>>(G, h0, h1, h2, pd.L[0], pd.L[1], pd.L[2], c->d_solvent, c->d_solute, u,
+                                          dim, dv);
+      CKL();
+      // B = beta (chi - 1) * ((c' + 1) dv): the Jacobian passes with slope
+      // c' + 1 and nothing subtracted (jacobian_t1 with its flag set)
+      pipeline<double, MODE_J>(c, dv, d1, pd.beta, 0.0, B);
+      const double bnorm = maxpy<double>(c, B, 1.0, {}, {}, true);
+      axpby<double, double>(c, 1.0, B, 0.0, Bc);  // the solvers may overwrite B
+      if (c->coarse) fgmres<double>(c, d, B, dT, 1e-11, 4000, restart);
+      else gmres<double>(c, d, B, dT, 1e-11, 4000, restart);
+      k_mu1<<<rb, 256, 0, c->stream>>>(G, T, c->v64, uc, dv, dT, pd.beta, pd.closure, c->d_charge,
+                                       part + (size_t)(3 * u + dim) * rb);
+      CKL();
+      // true residual of the solve: B - J dT (into dv, no longer needed)
+      eval_J<double>(c, d, dT, 1.0, dv, nullptr);
+      xpay<double, double, double>(c, Bc, -1.0, dv, dv);
+      const double rn = maxpy<double>(c, dv, 1.0, {}, {}, true);
+      if (bnorm > 0) worst = std::max(worst, rn / bnorm);
+    }
+  gr->adjoint_jv = c->jv_evals - jv0;
+  gr->adjoint_resid = worst;
+  std::vector<double> hp((size_t)rb * 3 * n);
+  if (n > 0)
+    CK(cudaMemcpyAsync(hp.data(), part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaEventRecord(e1, c->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  gr->seconds = ms * 1e-3;
+  for (double *p : {d1, dv, B, Bc, dT, uc, part}) dfree(p);
+  // mu1 = rho h^3 / beta * sum (chempot1, hnc3d.c:627-650)
+  const double f = pd.rho * c->h3 / pd.beta;
+  if (gr->dx)
+    for (int q = 0; q < 3 * n; ++q) {
+      double a = 0.0;
+      for (int b = 0; b < rb; ++b) a += hp[(size_t)q * rb + b];
+      gr->dx[q] = a * f;
+    }
+  return RISM3D_OK;
+}
+
 // (Re)binds the solute: its device copy, the short-range field v (FP64 and
 // FP32) and the long-range field L; grid, chi tables and work buffers stay.
 void bind_solute(rism3d_ctx *c, int n, const rism3d_site *solute) {
@@ -2020,6 +2098,11 @@ int rism3d_jacobian_transpose_t1(rism3d_ctx *ctx, const double *T, const double 
 int rism3d_gradient(rism3d_ctx *ctx, const double *T, rism3d_grad *grad) {
   if (!ctx || !T || !grad) return RISM3D_ERR_ARG;
   return guard([&] { return gradient_impl(ctx, T, grad); });
+}
+
+int rism3d_response(rism3d_ctx *ctx, const double *T, rism3d_grad *grad) {
+  if (!ctx || !T || !grad) return RISM3D_ERR_ARG;
+  return guard([&] { return response_impl(ctx, T, grad); });
 }
 
 int rism3d_solute_grad(const rism3d_problem *pd, int m, const rism3d_site *solvent, int n,

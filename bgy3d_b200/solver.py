@@ -349,6 +349,15 @@ class RismContext:
                    "gradient")
         return _grad_dict(g, arrs)
 
+    def response(self, T):
+        """Linear-response dmu/dx [n][3] at a converged FP64 T (rism3d_response,
+        the reference's "free-energy-response"): {"x", "krylov-jv",
+        "resid", "seconds"}."""
+        g, arrs = _grad_struct(self.n)
+        _abi.check(_abi.lib().rism3d_response(self._h, self._check_vec(T, self._torch.float64), ctypes.byref(g)),
+                   "response")
+        return {"x": arrs["x"], "krylov-jv": g.adjoint_jv, "resid": g.adjoint_resid, "seconds": g.seconds}
+
     def observables(self, T, want_g=False):
         res = _abi.Result()
         g = self.zeros() if want_g else None

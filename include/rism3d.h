@@ -275,6 +275,20 @@ int rism3d_jacobian_transpose_t1(rism3d_ctx *ctx, const double *T, const double 
    rism3d_solute_grad. */
 int rism3d_gradient(rism3d_ctx *ctx, const double *T, rism3d_grad *grad);
 
+/* Linear-response derivatives dmu/dx_u[n][3] at a converged T (FP64
+   device pointer), as the `response` branch of hnc3d_solute_solve computes
+   them ("free-energy-response", hnc3d.c:1969-2135 with response_t1,
+   1366-1421): for each unit displacement of one site, dv = field1 (the LJ
+   and FULL capped Coulomb derivative, bgy3d-solutes.c:381-468), the linear
+   solve J dT = beta (chi - 1) * ((c' + 1) dv) from zero, and the
+   differential of the free-energy density (chempot1, hnc3d.c:627-650,
+   form1, closures.f90:615-653) with the long-range correlation held fixed.
+   Writes grad->dx only (dq, dsigma, depsilon are left alone);
+   grad->adjoint_jv = J.v products of all 3n solves, grad->adjoint_resid =
+   the largest ||beta K((c'+1)dv) - J dT||_2 / ||beta K((c'+1)dv)||_2, grad->
+   seconds = device time.  PY has no closure differential: RISM3D_ERR_UNSUPPORTED. */
+int rism3d_response(rism3d_ctx *ctx, const double *T, rism3d_grad *grad);
+
 /* Points per axis of the two-grid preconditioner's coarse grid, written to
    n[3] (zeros when the preconditioner is off). */
 int rism3d_coarse_grid(rism3d_ctx *ctx, int *n);

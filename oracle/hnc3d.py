@@ -10,6 +10,7 @@ FFTW's unnormalised r2c/c2r map onto scipy.fft rfftn / (N * irfftn).
 import numpy as np
 import scipy.fft
 import scipy.special
+import scipy.sparse.linalg as sla
 
 from . import closures as cl
 from . import newton
@@ -327,3 +328,39 @@ def solute_solve(N, L, beta, rho, closure, solvent, solute, chi, rmax, renorm=Tr
     out["iters"] = iters
     out["problem"] = P
     return out
+
+
+def response(P, T, rtol=1e-12, sites=None):
+    """Linear-response derivatives dmu/dR[n][3] at a converged T: the
+    ``response`` branch of hnc3d_solute_solve (hnc3d.c:1969-2135) with
+    response_t1 (hnc3d.c:1366-1421).
+
+    Per unit displacement of site u along dim: dv = field1 (bgy3d-solutes.c:
+    381-468, LJ plus the full capped Coulomb); B = beta (chi-1) * (f'(x) dv),
+    the flagged jacobian_t1 (hnc3d.c:1305-1330); J dT = B solved from zero;
+    dx = -beta dv + dT, dc = closure1(dx) - beta dv, dh = dc + dT; then
+    chempot1 (hnc3d.c:627-650) with cl = -beta q_i uc held fixed.  ``sites``
+    limits the rows computed (the others stay zero)."""
+    beta, rho = P.beta, P.rho
+    obs = P.observables(T)
+    x, h, c, clr = obs["x"], obs["h"], obs["c"], obs["cl"]
+    d = cl.closure_slope(P.closure, beta, P.v, T)
+    shape = T.shape
+    n = T.size
+    A = sla.LinearOperator((n, n), matvec=lambda v: P.jacobian_t1(T, v.reshape(shape)).ravel(),
+                           dtype=np.float64)
+    dE = np.zeros((len(P.solute), 3))
+    for u in (range(len(P.solute)) if sites is None else sites):
+        for dim in range(3):
+            dv = solute_field1(P.N, P.L, P.solvent, P.solute, u, dim)
+            B = beta * P.ifft(P.star(P.fft(d * dv + dv) * P.h3)) * (1.0 / P.L3)
+            dT, info = sla.gmres(A, B.ravel(), rtol=rtol, atol=0.0, restart=60, maxiter=200)
+            dT = dT.reshape(shape)
+            dx = -beta * dv + dT
+            dc = d * dx - beta * dv
+            dh = dc + dT
+            dens = np.zeros(shape[1:])
+            for i in range(P.m):
+                dens = dens + cl.form1(P.closure, x[i], dx[i], h[i], dh[i], c[i], dc[i], clr[i])
+            dE[u, dim] = rho * dens.sum() * P.h3 / beta
+    return dE

@@ -101,3 +101,28 @@ def test_interp_rule_matches_reference_formula():
         ip = i + 1 if i < 48 else i
         im = i - 1 if i > 1 else i
         assert gi == tab[i] + (tab[ip] - tab[im]) / (ip - im) * (ix - i)
+
+
+def test_response_is_the_derivative_when_uncharged(fixture_loader):
+    """The restated response branch (oracle.hnc3d.response) is a forward-mode
+    derivative: with no solute charges it must equal the central difference
+    of mu in a site coordinate."""
+    meta, arr = fixture_loader("water_hnc_n24")
+    s = meta["settings"]
+    sol = [dict(a, charge=0.0, x=tuple(a["x"])) for a in meta["solute"]]
+    N, L = (s["N"],) * 3, (2 * s["L"],) * 3
+
+    def solve(solute, T0=None):
+        return hnc3d.solute_solve(N, L, s["beta"], s["rho"], s["closure"], meta["solvent"], solute, arr["chi"],
+                                  s["rmax"], tol=1e-12, T0=T0)
+
+    out = solve(sol)
+    dE = hnc3d.response(out["problem"], out["T"], sites=[0])
+    h = 1e-4
+    mu = []
+    for sgn in (1, -1):
+        moved = [dict(a) for a in sol]
+        moved[0]["x"] = (sol[0]["x"][0] + sgn * h,) + sol[0]["x"][1:]
+        mu.append(solve(moved, out["T"])["mu"])
+    fd = (mu[0] - mu[1]) / (2 * h)
+    assert abs(dE[0, 0] - fd) < 1e-6 * max(1.0, abs(fd))
