@@ -226,7 +226,11 @@ def renorm_kernel(solvent, chi, rmax, alpha=G):
 class Problem:
     """Everything hnc3d_solute_solve sets up before SNES (hnc3d.c:1790-1966)."""
 
-    def __init__(self, N, L, beta, rho, closure, solvent, solute, chi, rmax, renorm=True):
+    def __init__(self, N, L, beta, rho, closure, solvent, solute, chi, rmax, renorm=True, chi3=None):
+        """chi: [m][m][nrad] radial chi table, or None with chi3 = chi - 1 on
+        the k grid (packed pairs [m(m+1)/2][N2][N1][N0/2+1], complex), the
+        --solvent-3d kernel read from x%d%d-fft.bin (solvent_kernel_file,
+        hnc3d.c:1432-1437), which implies the no-renorm form (1575-1587)."""
         self.N = tuple(int(n) for n in N)
         self.L = tuple(float(l) for l in L)
         self.h = tuple(self.L[d] / self.N[d] for d in range(3))
@@ -236,16 +240,25 @@ class Problem:
         self.renorm = renorm
         self.h3 = self.h[0] * self.h[1] * self.h[2]
         self.L3 = self.L[0] * self.L[1] * self.L[2]
-        nrad = chi.shape[-1]
-        dk = np.pi / rmax
         kk = kabs(self.N, self.L)
         m = self.m
-        self.chi_fft = np.zeros((m, m) + kk.shape)
-        for i in range(m):
-            for j in range(i + 1):
-                tab = chi[i, j] - (1.0 if i == j else 0.0)
-                self.chi_fft[i, j] = interp(kk, tab, dk)
-                self.chi_fft[j, i] = self.chi_fft[i, j]
+        if chi3 is not None:
+            renorm = self.renorm = False
+            self.chi_fft = np.zeros((m, m) + kk.shape, dtype=complex)
+            p = 0
+            for i in range(m):
+                for j in range(i + 1):
+                    self.chi_fft[i, j] = self.chi_fft[j, i] = chi3[p]
+                    p += 1
+        else:
+            nrad = chi.shape[-1]
+            dk = np.pi / rmax
+            self.chi_fft = np.zeros((m, m) + kk.shape)
+            for i in range(m):
+                for j in range(i + 1):
+                    tab = chi[i, j] - (1.0 if i == j else 0.0)
+                    self.chi_fft[i, j] = interp(kk, tab, dk)
+                    self.chi_fft[j, i] = self.chi_fft[i, j]
         self.charge = np.array([s["charge"] for s in solvent])
         F = form_factor_centered(self.N, self.L, solute)
         if renorm:
@@ -316,9 +329,9 @@ class Problem:
 
 
 def solute_solve(N, L, beta, rho, closure, solvent, solute, chi, rmax, renorm=True,
-                 tol=1e-12, T0=None, picard_steps=0, verbose=False):
+                 tol=1e-12, T0=None, picard_steps=0, verbose=False, chi3=None):
     """hnc3d_solute_solve (hnc3d.c:1762-2350) returning mu, PMV, g, T."""
-    P = Problem(N, L, beta, rho, closure, solvent, solute, chi, rmax, renorm)
+    P = Problem(N, L, beta, rho, closure, solvent, solute, chi, rmax, renorm, chi3=chi3)
     T0 = np.zeros((P.m, P.N[2], P.N[1], P.N[0])) if T0 is None else T0
     jv = P.jacobian_t1 if closure != cl.PY else None
     T, iters = newton.solve(P.iterate_t1, T0, jv=jv, tol=tol, picard_steps=picard_steps,
