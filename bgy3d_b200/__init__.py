@@ -7,5 +7,5 @@ access to the residual and Jacobian (``RismContext``).
 """
 from ._abi import CLOSURES, RismError, lib  # noqa: F401
 from .sites import MOLECULES, find_molecule, synthetic_solute  # noqa: F401
-from .solver import (DEFAULTS, RismContext, hnc3d_run_batch, hnc3d_run_solute, hnc3d_solute_grad,  # noqa: F401
-                     problem_data, rism_solvent)
+from .solver import (DEFAULTS, RismContext, hnc3d_run_batch, hnc3d_run_solute, hnc3d_run_solvent,  # noqa: F401
+                     hnc3d_solute_grad, problem_data, rism_solvent)

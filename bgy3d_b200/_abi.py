@@ -67,6 +67,14 @@ class Grad(ctypes.Structure):
                 ("adjoint_jv", ctypes.c_int), ("adjoint_resid", ctypes.c_double), ("seconds", ctypes.c_double)]
 
 
+class SolventResult(ctypes.Structure):
+    _fields_ = [("mu", ctypes.c_double), ("mu_hnc", ctypes.c_double), ("mu_kh", ctypes.c_double),
+                ("mu_gf", ctypes.c_double), ("a", ctypes.c_double), ("kappa", ctypes.c_double),
+                ("resid_inf", ctypes.c_double), ("resid_2", ctypes.c_double), ("status", ctypes.c_int),
+                ("newton_iters", ctypes.c_int), ("f_evals", ctypes.c_int), ("jv_evals", ctypes.c_int),
+                ("seconds", ctypes.c_double)]
+
+
 # Every entry point declared in include/rism3d.h (checked by the CPU tests).
 EXPORTS = [
     "rism3d_problem_defaults", "rism3d_solute_solve", "rism3d_ctx_create",
@@ -76,7 +84,8 @@ EXPORTS = [
     "rism3d_profile", "rism1d_solvent_chi", "rism3d_jacobian_apply_noalloc",
     "rism3d_precondition", "rism3d_coarse_grid", "rism3d_solve_batch",
     "rism3d_solute_grad", "rism3d_gradient", "rism3d_jacobian_transpose_t1", "rism3d_ctx_set_solute",
-    "rism3d_response",
+    "rism3d_response", "rism3d_solvent_solve", "rism3d_solvent_ctx_create", "rism3d_ctx_create_chi3",
+    "rism3d_solute_solve_chi3",
 ]
 
 _lib = None
@@ -137,6 +146,14 @@ def lib():
     L.rism3d_ctx_set_solute.restype = I
     L.rism3d_response.argtypes = [V, V, P(Grad)]
     L.rism3d_response.restype = I
+    L.rism3d_solvent_solve.argtypes = [P(Problem), I, P(Site), P(D), P(D), P(D), P(D), P(SolventResult)]
+    L.rism3d_solvent_solve.restype = I
+    L.rism3d_solvent_ctx_create.argtypes = [P(Problem), I, P(Site), P(V)]
+    L.rism3d_solvent_ctx_create.restype = I
+    L.rism3d_ctx_create_chi3.argtypes = [P(Problem), I, P(Site), I, P(Site), P(D), P(V)]
+    L.rism3d_ctx_create_chi3.restype = I
+    L.rism3d_solute_solve_chi3.argtypes = [P(Problem), I, P(Site), I, P(Site), P(D), P(D), P(D), P(Result)]
+    L.rism3d_solute_solve_chi3.restype = I
     _lib = L
     return L
 

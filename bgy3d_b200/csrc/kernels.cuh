@@ -235,6 +235,7 @@ template <typename T> struct ZParams {
   const typename Vec2<T>::type *chi;   // [m(m+1)/2][nrad] (value, slope) of chi-1
   const typename Vec2<T>::type *stab;  // [m][nrad] (value, slope) of beta/eps0 s_i, or null
   const typename Cx<T>::type *L;       // [N2][N1][Nhp] long-range field / h^3, or null
+  const typename Cx<T>::type *chi3;    // chi - 1 on the k grid [m(m+1)/2][N2][N1][Nhp], or null
   int nrad;
   double dkr;                          // pi / rmax
   T a[kMaxSites];                      // c_j -= a_j L      (no-renorm: beta q_j)
@@ -290,10 +291,14 @@ __global__ void __launch_bounds__(256) k_z(Geo g, AxisPlan pz, typename Cx<T>::t
     const int kz = kfreq(z, N2);
     const double k0 = kx * g.dk0, k2 = kz * g.dk2;
     const double kk = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(k0, k0), __dmul_rn(k1, k1)), __dmul_rn(k2, k2)));
-    const double ix = kk / zp.dkr - 0.5;
-    int i = (int)(ix + 0.5);
-    i = min(max(i, 0), zp.nrad - 1);
-    const T fr = T(ix - i);
+    int i = 0;
+    T fr = T(0);
+    if (zp.chi3 == nullptr) {
+      const double ix = kk / zp.dkr - 0.5;
+      i = (int)(ix + 0.5);
+      i = min(max(i, 0), zp.nrad - 1);
+      fr = T(ix - i);
+    }
     V c[kMaxSites];
 #pragma unroll
     for (int j = 0; j < kMaxSites; ++j)
@@ -315,10 +320,16 @@ __global__ void __launch_bounds__(256) k_z(Geo g, AxisPlan pz, typename Cx<T>::t
       for (int j = 0; j < kMaxSites; ++j) {
         if (j >= m) break;
         const int pidx = ii >= j ? ii * (ii + 1) / 2 + j : j * (j + 1) / 2 + ii;
-        const P2 tv = zp.chi[(long long)pidx * zp.nrad + i];
-        const T x = tv.x + tv.y * fr;
-        t.x += x * c[j].x;
-        t.y += x * c[j].y;
+        if (zp.chi3 != nullptr) {  // complex chi - 1 of the 3D solvent
+          const V x = zp.chi3[(long long)pidx * g.Nc + z * zstride + col + b];
+          t.x += x.x * c[j].x - x.y * c[j].y;
+          t.y += x.x * c[j].y + x.y * c[j].x;
+        } else {
+          const P2 tv = zp.chi[(long long)pidx * zp.nrad + i];
+          const T x = tv.x + tv.y * fr;
+          t.x += x * c[j].x;
+          t.y += x * c[j].y;
+        }
       }
       if (MODE == MODE_F && zp.L != nullptr) {
         T bb = zp.bconst[ii];

@@ -28,6 +28,7 @@
 #include "grad.cuh"
 #include "krylov.cuh"
 #include "rism3d.h"
+#include "solvent.cuh"
 #include "twogrid.cuh"
 #include "twogrid_fft.cuh"
 
@@ -194,6 +195,13 @@ struct rism3d_ctx {
   float2 *L32 = nullptr;
   double2 *chi64 = nullptr, *s64 = nullptr;
   float2 *chi32 = nullptr, *s32 = nullptr;
+  double2 *chi3_64 = nullptr;  // chi - 1 on the k grid (W layout, packed pairs), or null
+  float2 *chi3_32 = nullptr;
+  // pure-solvent context: solvent sites (0 for a solute context), the pair
+  // constants of its OZ z pass and C(k) at the last residual's point
+  int pure = 0;
+  std::vector<double> pq2, pwr;
+  double2 *ck = nullptr;
   void *W = nullptr;  // complex work buffer, FP64-sized, reused by the FP32 path
   SiteP *d_solute = nullptr, *d_solvent = nullptr;
   int n_cap = 0;  // capacity of d_solute
@@ -249,7 +257,7 @@ struct rism3d_ctx {
     auto fr = [](void *p) { dfree(p); };
     for (int i = 0; i < 3; ++i) { fr(tw64[i]); fr(tw32[i]); }
     fr(post64); fr(post32); fr(v64); fr(v32); fr(L64); fr(L32);
-    fr(chi64); fr(s64); fr(chi32); fr(s32); fr(W); fr(d_solute); fr(d_solvent); fr(d_charge);
+    fr(chi64); fr(s64); fr(chi32); fr(s32); fr(chi3_64); fr(chi3_32); fr(ck); fr(W); fr(d_solute); fr(d_solvent); fr(d_charge);
     fr(npart); fr(dpart); fr(dres); fr(F64); fr(X64t); fr(F64t); fr(X32); fr(F32); fr(X32t); fr(F32t);
     fr(d64); fr(d32); fr(dx64); fr(dx32); fr(d_err);
     for (auto p : basis64) fr(p);
@@ -300,11 +308,12 @@ template <typename T> ZParams<T> zparams(rism3d_ctx *c, bool full);
 template <> ZParams<double> zparams<double>(rism3d_ctx *c, bool full) {
   ZParams<double> z{};
   z.chi = c->chi64;
+  z.chi3 = c->chi3_64;
   z.stab = (full && c->pd.renorm) ? c->s64 : nullptr;
   z.L = full ? c->L64 : nullptr;
   z.nrad = c->pd.nrad;
   z.dkr = c->dkr;
-  for (int i = 0; i < c->m; ++i) {
+  for (int i = 0; i < c->m && !c->pure; ++i) {
     z.a[i] = c->pd.renorm ? 0.0 : c->pd.beta * c->charge[i];
     z.bconst[i] = c->pd.renorm ? 0.0 : c->pd.beta * c->charge[i];
   }
@@ -313,11 +322,12 @@ template <> ZParams<double> zparams<double>(rism3d_ctx *c, bool full) {
 template <> ZParams<float> zparams<float>(rism3d_ctx *c, bool full) {
   ZParams<float> z{};
   z.chi = c->chi32;
+  z.chi3 = c->chi3_32;
   z.stab = (full && c->pd.renorm) ? c->s32 : nullptr;
   z.L = full ? c->L32 : nullptr;
   z.nrad = c->pd.nrad;
   z.dkr = c->dkr;
-  for (int i = 0; i < c->m; ++i) {
+  for (int i = 0; i < c->m && !c->pure; ++i) {
     z.a[i] = c->pd.renorm ? 0.f : (float)(c->pd.beta * c->charge[i]);
     z.bconst[i] = c->pd.renorm ? 0.f : (float)(c->pd.beta * c->charge[i]);
   }
@@ -428,8 +438,57 @@ template <typename T, bool INV> void launch_y(rism3d_ctx *c) {
   CKL();
 }
 
+void allow_smem(const void *fn, size_t need);
+
+// z pass of a pure-solvent context (solvent.cuh), FP64, for MS solvent sites.
+template <int MODE, int MS> void launch_oz_ms(rism3d_ctx *c) {
+  PureParams<MS> pp{};
+  pp.rho = c->pd.rho;
+  pp.beta = c->pd.beta;
+  pp.h3 = c->h3;
+  pp.ck = c->ck;
+  for (int p = 0; p < PureParams<MS>::NP; ++p) {
+    pp.q2[p] = c->pq2[p];
+    pp.wr[p] = c->pwr[p];
+  }
+  const int B = c->tl<double>().BZ;
+  dim3 grid((c->g.Nh + B - 1) / B, c->g.N1);
+  const size_t sm = zsmem<double>(c);
+  auto *W = c->work<double>();
+  if (B == 16) k_z_oz<MODE, 16, MS><<<grid, 256, sm, c->stream>>>(c->g, c->plan<double>(2), W, pp);
+  else if (B == 8) k_z_oz<MODE, 8, MS><<<grid, 256, sm, c->stream>>>(c->g, c->plan<double>(2), W, pp);
+  else k_z_oz<MODE, 4, MS><<<grid, 256, sm, c->stream>>>(c->g, c->plan<double>(2), W, pp);
+  CKL();
+}
+template <int MODE> void launch_oz(rism3d_ctx *c) {
+  switch (c->pure) {
+    case 1: launch_oz_ms<MODE, 1>(c); break;
+    case 2: launch_oz_ms<MODE, 2>(c); break;
+    case 3: launch_oz_ms<MODE, 3>(c); break;
+    default: launch_oz_ms<MODE, 4>(c); break;
+  }
+}
+template <int MODE, int MS> void allow_oz_ms(size_t need) {
+  allow_smem((const void *)k_z_oz<MODE, 16, MS>, need);
+  allow_smem((const void *)k_z_oz<MODE, 8, MS>, need);
+  allow_smem((const void *)k_z_oz<MODE, 4, MS>, need);
+}
+template <int MS> void allow_oz(size_t need) {
+  allow_oz_ms<MODE_F, MS>(need);
+  allow_oz_ms<MODE_J, MS>(need);
+  allow_oz_ms<MODE_VL, MS>(need);
+}
+
 template <typename T, int MODE> void launch_z(rism3d_ctx *c) {
   TimeScope ts(c, TK_Z, sizeof(T) == 8 ? 0 : 1);
+  if (c->pure) {
+    if constexpr (sizeof(T) == 8 && (MODE == MODE_F || MODE == MODE_J)) {
+      launch_oz<MODE>(c);
+      return;
+    }
+    g_last_error = "pure-solvent passes are FP64 residual and Jacobian only";
+    throw ArgFail{RISM3D_ERR_UNSUPPORTED, g_last_error};
+  }
   auto *W = c->work<T>();
   const ZParams<T> zp = zparams<T>(c, MODE == MODE_F);
   if (c->stat[sizeof(T) == 8 ? 0 : 1]) {
@@ -1529,130 +1588,232 @@ void bind_solute(rism3d_ctx *c, int n, const rism3d_site *solute) {
   if (c->coarse) bind_solute(c->coarse, n, solute);
 }
 
-int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int n, const rism3d_site *solute,
-                const double *chi, rism3d_ctx **out) {
-  if (!pd || !solvent || (!solute && n > 0) || !chi || !out) throw ArgFail{RISM3D_ERR_ARG, "null argument"};
-  if (m < 1 || m > kMaxSites) throw ArgFail{RISM3D_ERR_ARG, "solvent sites must be 1..6"};
-  if (n < 0) throw ArgFail{RISM3D_ERR_ARG, "negative solute size"};
+void check_grid(const rism3d_problem *pd) {
   for (int d = 0; d < 3; ++d) {
     if (!is_2a3b(pd->N[d]) || pd->N[d] % 2 || pd->N[d] < 8 || pd->N[d] > kMaxN)
       throw ArgFail{RISM3D_ERR_ARG, "N must be even 2^a 3^b in [8, 512]"};
     if (!(pd->L[d] > 0)) throw ArgFail{RISM3D_ERR_ARG, "L must be positive"};
   }
-  if (pd->nrad < 4 || !(pd->rmax > 0)) throw ArgFail{RISM3D_ERR_ARG, "bad radial grid"};
   if (pd->closure < 0 || pd->closure > RISM3D_PSE7) throw ArgFail{RISM3D_ERR_ARG, "no such closure"};
+}
+
+// Geometry, tile shapes, FFT plans and twiddles of a context over `fields`
+// real fields on the grid of c->pd.
+void init_grid(rism3d_ctx *c, int fields) {
+  const rism3d_problem *pd = &c->pd;
+  Geo &G = c->g;
+  G.N0 = pd->N[0]; G.N1 = pd->N[1]; G.N2 = pd->N[2];
+  G.M = G.N0 / 2;
+  G.Nh = G.M + 1;
+  G.Nhp = (G.Nh + 1) & ~1;
+  G.m = fields;
+  G.Nr = (long long)G.N0 * G.N1 * G.N2;
+  G.Nc = (long long)G.Nhp * G.N1 * G.N2;
+  const double pi = 3.14159265358979323846;
+  G.dk0 = 2 * pi / pd->L[0];
+  G.dk1 = 2 * pi / pd->L[1];
+  G.dk2 = 2 * pi / pd->L[2];
+  c->nvec = (long long)fields * G.Nr;
+  const double h0 = pd->L[0] / pd->N[0], h1 = pd->L[1] / pd->N[1], h2 = pd->L[2] / pd->N[2];
+  c->h3 = h0 * h1 * h2;
+  c->dkr = pd->rmax > 0 ? pi / pd->rmax : 0.0;
+  const int m = fields;
+  // tile shapes per precision: n * batch <= reg_complex * 256 threads
+  for (int pr = 0; pr < 2; ++pr) {
+    const int rc = pr == 0 ? reg_complex<double2>() : reg_complex<float2>();
+    TileShape &t = c->tiles[pr];
+    t.RX = 32;
+    while (t.RX > 1 && G.M * t.RX > rc * 256) t.RX /= 2;
+    t.BY = 16;
+    while (t.BY > 4 && G.N1 * t.BY > rc * 256) t.BY /= 2;
+    t.BZ = 16;
+    while (t.BZ > 4 && G.N2 * t.BZ > rc * 256) t.BZ /= 2;
+    if (G.N1 * t.BY > rc * 256 || G.N2 * t.BZ > rc * 256)
+      throw ArgFail{RISM3D_ERR_ARG, "grid too large for the tile shapes"};
+    // small grids (the coarse problem): smaller batches while a pass would
+    // otherwise launch fewer than two CTAs per SM
+    const long long want = 2 * 148;
+    while (t.RX > 4 && (long long)((G.N1 * G.N2 + t.RX - 1) / t.RX) * m < want) t.RX /= 2;
+    while (t.BY > 4 && (long long)((G.Nh + t.BY - 1) / t.BY) * G.N2 * m < want) t.BY /= 2;
+    while (t.BZ > 4 && (long long)((G.Nh + t.BZ - 1) / t.BZ) * G.N1 < want) t.BZ /= 2;
+    // the z tile holds every field's columns: at most 200 KB of shared memory
+    const size_t cs = pr == 0 ? sizeof(double2) : sizeof(float2);
+    while (t.BZ > 4 && cs * (size_t)G.N2 * (size_t)(m * t.BZ + 1) > 200 * 1024) t.BZ /= 2;
+  }
+  // FFT plans and twiddles
+  const int lens[3] = {G.M, G.N1, G.N2};
+  for (int a = 0; a < 3; ++a) {
+    std::vector<double2> t64;
+    std::vector<float2> t32;
+    twiddles(lens[a], t64, t32);
+    c->tw64[a] = dalloc<double2>(lens[a]);
+    c->tw32[a] = dalloc<float2>(lens[a]);
+    CK(cudaMemcpy(c->tw64[a], t64.data(), sizeof(double2) * lens[a], cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->tw32[a], t32.data(), sizeof(float2) * lens[a], cudaMemcpyHostToDevice));
+  }
+  c->px64 = make_plan(G.M); c->px64.tw = c->tw64[0];
+  c->py64 = make_plan(G.N1); c->py64.tw = c->tw64[1];
+  c->pz64 = make_plan(G.N2); c->pz64.tw = c->tw64[2];
+  c->px32 = c->px64; c->px32.tw = c->tw32[0];
+  c->py32 = c->py64; c->py32.tw = c->tw32[1];
+  c->pz32 = c->pz64; c->pz32.tw = c->tw32[2];
+  {
+    std::vector<double2> t64;
+    std::vector<float2> t32;
+    twiddles(G.N0, t64, t32);  // post twiddles exp(-2 pi i k / N0), k in [0, M]
+    c->post64 = dalloc<double2>(G.Nh);
+    c->post32 = dalloc<float2>(G.Nh);
+    CK(cudaMemcpy(c->post64, t64.data(), sizeof(double2) * G.Nh, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->post32, t32.data(), sizeof(float2) * G.Nh, cudaMemcpyHostToDevice));
+  }
+}
+
+// The complex work buffer, the reduction partials and the wait-error flag.
+void init_work(rism3d_ctx *c) {
+  const Geo &G = c->g;
+  c->W = dalloc<double2>((size_t)G.m * G.Nc);
+  // reduction blocks: about four 16-byte loads per thread, at most 4 per SM
+  c->red_blocks = (int)std::min<long long>(592, std::max<long long>(8, (c->nvec / 4 + 1023) / 1024));
+  c->dpart = dalloc<double>((size_t)c->red_blocks * kVecMax + 64);
+  c->dres = dalloc<double>(4 * kVecMax);
+  const int rows = G.N1 * G.N2;
+  const int rxmin = std::min(std::min(c->tiles[0].RX, c->tiles[1].RX), kStaticRX);
+  c->npart = dalloc<NormPartial>((size_t)((rows + rxmin - 1) / rxmin) * G.m);
+  c->d_err = dalloc<int>(1);
+  CK(cudaMemset(c->d_err, 0, sizeof(int)));
+}
+
+// Shared-memory opt-in: a kernel may use the device's per-block opt-in limit
+// minus its own static shared memory, which must cover `need` bytes.
+void allow_smem(const void *fn, size_t need) {
+  int dev = 0, optin = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa{};
+  CK(cudaFuncGetAttributes(&fa, fn));
+  const int dyn = optin - (int)fa.sharedSizeBytes;
+  if ((size_t)dyn < need) throw ArgFail{RISM3D_ERR_ARG, "tile exceeds shared memory"};
+  CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+}
+
+// Largest dynamic shared memory of the runtime-length passes.
+size_t generic_smem(rism3d_ctx *c) {
+  size_t need = 0;
+  for (size_t b : {xsmem<double>(c), ysmem<double>(c), zsmem<double>(c), xsmem<float>(c), ysmem<float>(c),
+                   zsmem<float>(c)})
+    need = std::max(need, b);
+  return need;
+}
+
+// Opt-in for the runtime-length x and y passes (every context uses them).
+void allow_xy(size_t need) {
+  allow_smem((const void *)k_xfwd<double, MODE_F>, need);
+  allow_smem((const void *)k_xfwd<double, MODE_J>, need);
+  allow_smem((const void *)k_xfwd<float, MODE_F>, need);
+  allow_smem((const void *)k_xfwd<float, MODE_J>, need);
+  allow_smem((const void *)k_xinv<double>, need);
+  allow_smem((const void *)k_xinv<float>, need);
+  allow_smem((const void *)k_xfwd<double, MODE_FWD>, need);
+#define OPTIN_Y(T)                                          \
+  allow_smem((const void *)k_y<T, false, 16>, need);        \
+  allow_smem((const void *)k_y<T, true, 16>, need);         \
+  allow_smem((const void *)k_y<T, false, 8>, need);         \
+  allow_smem((const void *)k_y<T, true, 8>, need);          \
+  allow_smem((const void *)k_y<T, false, 4>, need);         \
+  allow_smem((const void *)k_y<T, true, 4>, need);
+  OPTIN_Y(double)
+  OPTIN_Y(float)
+#undef OPTIN_Y
+}
+
+// chi3 (optional): chi - 1 on the k grid, packed pairs of complex
+// [m(m+1)/2][N2][N1][N0/2+1] (the --solvent-3d kernel); then chi is unused,
+// the long-range term takes the no-renorm form and the passes are the
+// runtime-length ones without the two-grid preconditioner.
+int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int n, const rism3d_site *solute,
+                const double *chi, const double *chi3, rism3d_ctx **out) {
+  if (!pd || !solvent || (!solute && n > 0) || (!chi && !chi3) || !out) throw ArgFail{RISM3D_ERR_ARG, "null argument"};
+  if (m < 1 || m > kMaxSites) throw ArgFail{RISM3D_ERR_ARG, "solvent sites must be 1..6"};
+  if (n < 0) throw ArgFail{RISM3D_ERR_ARG, "negative solute size"};
+  check_grid(pd);
+  if (!chi3 && (pd->nrad < 4 || !(pd->rmax > 0))) throw ArgFail{RISM3D_ERR_ARG, "bad radial grid"};
   auto c = new rism3d_ctx();
   try {
     c->pd = *pd;
+    if (chi3) {
+      c->pd.renorm = 0;
+      c->pd.coarse_h = 0;
+    }
+    pd = &c->pd;
     c->m = m;
     c->n = n;
     c->solvent.assign(solvent, solvent + m);
     c->solute.assign(solute, solute + n);
-    Geo &G = c->g;
-    G.N0 = pd->N[0]; G.N1 = pd->N[1]; G.N2 = pd->N[2];
-    G.M = G.N0 / 2;
-    G.Nh = G.M + 1;
-    G.Nhp = (G.Nh + 1) & ~1;
-    G.m = m;
-    G.Nr = (long long)G.N0 * G.N1 * G.N2;
-    G.Nc = (long long)G.Nhp * G.N1 * G.N2;
     const double pi = 3.14159265358979323846;
-    G.dk0 = 2 * pi / pd->L[0];
-    G.dk1 = 2 * pi / pd->L[1];
-    G.dk2 = 2 * pi / pd->L[2];
-    c->nvec = (long long)m * G.Nr;
-    const double h0 = pd->L[0] / pd->N[0], h1 = pd->L[1] / pd->N[1], h2 = pd->L[2] / pd->N[2];
-    c->h3 = h0 * h1 * h2;
-    c->dkr = pi / pd->rmax;
-    // tile shapes per precision: n * batch <= reg_complex * 256 threads
-    for (int pr = 0; pr < 2; ++pr) {
-      const int rc = pr == 0 ? reg_complex<double2>() : reg_complex<float2>();
-      TileShape &t = c->tiles[pr];
-      t.RX = 32;
-      while (t.RX > 1 && G.M * t.RX > rc * 256) t.RX /= 2;
-      t.BY = 16;
-      while (t.BY > 4 && G.N1 * t.BY > rc * 256) t.BY /= 2;
-      t.BZ = 16;
-      while (t.BZ > 4 && G.N2 * t.BZ > rc * 256) t.BZ /= 2;
-      if (G.N1 * t.BY > rc * 256 || G.N2 * t.BZ > rc * 256)
-        throw ArgFail{RISM3D_ERR_ARG, "grid too large for the tile shapes"};
-      // small grids (the coarse problem): smaller batches while a pass would
-      // otherwise launch fewer than two CTAs per SM
-      const long long want = 2 * 148;
-      while (t.RX > 4 && (long long)((G.N1 * G.N2 + t.RX - 1) / t.RX) * m < want) t.RX /= 2;
-      while (t.BY > 4 && (long long)((G.Nh + t.BY - 1) / t.BY) * G.N2 * m < want) t.BY /= 2;
-      while (t.BZ > 4 && (long long)((G.Nh + t.BZ - 1) / t.BZ) * G.N1 < want) t.BZ /= 2;
+    if (!chi3) {
+      // |k| of every grid point must fall inside the chi table (interp
+      // assert, bgy3d-vec.c:30-31); checked before any device work
+      const double dk[3] = {2 * pi / pd->L[0], 2 * pi / pd->L[1], 2 * pi / pd->L[2]};
+      const double kmax = std::sqrt(std::pow(pd->N[0] / 2 * dk[0], 2) + std::pow(pd->N[1] / 2 * dk[1], 2) +
+                                    std::pow(pd->N[2] / 2 * dk[2], 2));
+      if ((int)(kmax / (pi / pd->rmax) - 0.5 + 0.5) >= pd->nrad) throw ArgFail{RISM3D_ERR_TABLE, "chi table too short"};
     }
-    // |k| of every grid point must fall inside the chi table (interp assert,
-    // bgy3d-vec.c:30-31)
-    const double kmax = std::sqrt(std::pow(G.M * G.dk0, 2) + std::pow(G.N1 / 2 * G.dk1, 2) +
-                                  std::pow(G.N2 / 2 * G.dk2, 2));
-    if ((int)(kmax / c->dkr - 0.5 + 0.5) >= pd->nrad) throw ArgFail{RISM3D_ERR_TABLE, "chi table too short"};
+    init_grid(c, m);
+    const Geo &G = c->g;
     for (int i = 0; i < m; ++i) c->charge.push_back(solvent[i].charge);
 
-    // FFT plans and twiddles
-    const int lens[3] = {G.M, G.N1, G.N2};
-    for (int a = 0; a < 3; ++a) {
-      std::vector<double2> t64;
-      std::vector<float2> t32;
-      twiddles(lens[a], t64, t32);
-      c->tw64[a] = dalloc<double2>(lens[a]);
-      c->tw32[a] = dalloc<float2>(lens[a]);
-      CK(cudaMemcpy(c->tw64[a], t64.data(), sizeof(double2) * lens[a], cudaMemcpyHostToDevice));
-      CK(cudaMemcpy(c->tw32[a], t32.data(), sizeof(float2) * lens[a], cudaMemcpyHostToDevice));
-    }
-    c->px64 = make_plan(G.M); c->px64.tw = c->tw64[0];
-    c->py64 = make_plan(G.N1); c->py64.tw = c->tw64[1];
-    c->pz64 = make_plan(G.N2); c->pz64.tw = c->tw64[2];
-    c->px32 = c->px64; c->px32.tw = c->tw32[0];
-    c->py32 = c->py64; c->py32.tw = c->tw32[1];
-    c->pz32 = c->pz64; c->pz32.tw = c->tw32[2];
-    {
-      std::vector<double2> t64;
-      std::vector<float2> t32;
-      twiddles(G.N0, t64, t32);  // post twiddles exp(-2 pi i k / N0), k in [0, M]
-      c->post64 = dalloc<double2>(G.Nh);
-      c->post32 = dalloc<float2>(G.Nh);
-      CK(cudaMemcpy(c->post64, t64.data(), sizeof(double2) * G.Nh, cudaMemcpyHostToDevice));
-      CK(cudaMemcpy(c->post32, t32.data(), sizeof(float2) * G.Nh, cudaMemcpyHostToDevice));
-    }
-    // radial tables: chi - delta (solvent_kernel_rism, hnc3d.c:1548-1556) and
-    // beta/eps0 s_i (rism_solvent_renorm, rism.f90:141-208)
-    const int nrad = pd->nrad;
     const int npair = m * (m + 1) / 2;
-    std::vector<double2> chi64((size_t)npair * nrad), s64((size_t)m * nrad);
-    std::vector<double> tab(nrad);
-    std::vector<double2> pr;
-    for (int i = 0; i < m; ++i)
-      for (int j = 0; j <= i; ++j) {
-        for (int k = 0; k < nrad; ++k) tab[k] = chi[((size_t)i * m + j) * nrad + k] - (i == j ? 1.0 : 0.0);
+    if (chi3) {
+      // chi - 1 on the k grid into the padded W layout [pair][N2][N1][Nhp]
+      const size_t rows = (size_t)npair * G.N2 * G.N1;
+      c->chi3_64 = dalloc<double2>((size_t)npair * G.Nc);
+      c->chi3_32 = dalloc<float2>((size_t)npair * G.Nc);
+      CK(cudaMemset(c->chi3_64, 0, sizeof(double2) * (size_t)npair * G.Nc));
+      CK(cudaMemset(c->chi3_32, 0, sizeof(float2) * (size_t)npair * G.Nc));
+      CK(cudaMemcpy2D(c->chi3_64, sizeof(double2) * G.Nhp, chi3, sizeof(double2) * G.Nh, sizeof(double2) * G.Nh,
+                      rows, cudaMemcpyHostToDevice));
+      std::vector<float2> h32(rows * G.Nh);
+      for (size_t q = 0; q < h32.size(); ++q) h32[q] = make_float2((float)chi3[2 * q], (float)chi3[2 * q + 1]);
+      CK(cudaMemcpy2D(c->chi3_32, sizeof(float2) * G.Nhp, h32.data(), sizeof(float2) * G.Nh, sizeof(float2) * G.Nh,
+                      rows, cudaMemcpyHostToDevice));
+    } else {
+      // radial tables: chi - delta (solvent_kernel_rism, hnc3d.c:1548-1556) and
+      // beta/eps0 s_i (rism_solvent_renorm, rism.f90:141-208)
+      const int nrad = pd->nrad;
+      std::vector<double2> chi64((size_t)npair * nrad), s64((size_t)m * nrad);
+      std::vector<double> tab(nrad);
+      std::vector<double2> pr;
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j <= i; ++j) {
+          for (int k = 0; k < nrad; ++k) tab[k] = chi[((size_t)i * m + j) * nrad + k] - (i == j ? 1.0 : 0.0);
+          interp_pairs(tab.data(), nrad, pr);
+          std::copy(pr.begin(), pr.end(), chi64.begin() + (size_t)(i * (i + 1) / 2 + j) * nrad);
+        }
+      const double dk = pi / pd->rmax;
+      for (int i = 0; i < m; ++i) {
+        std::vector<double> x(nrad, 0.0);
+        for (int j = 0; j < m; ++j)
+          for (int k = 0; k < nrad; ++k) x[k] = x[k] + chi[((size_t)j * m + i) * nrad + k] * solvent[j].charge;
+        for (int k = 0; k < nrad; ++k) {
+          const double kk = (2 * (k + 1) - 1) * dk / 2;
+          const double v = kk == 0.0 ? 0.0 : 4 * pi * std::exp(-kk * kk / (4 * kG * kG)) / (kk * kk);
+          tab[k] = pd->beta * kEps0Inv * (x[k] * v);
+        }
         interp_pairs(tab.data(), nrad, pr);
-        std::copy(pr.begin(), pr.end(), chi64.begin() + (size_t)(i * (i + 1) / 2 + j) * nrad);
+        std::copy(pr.begin(), pr.end(), s64.begin() + (size_t)i * nrad);
       }
-    const double dk = pi / pd->rmax;
-    for (int i = 0; i < m; ++i) {
-      std::vector<double> x(nrad, 0.0);
-      for (int j = 0; j < m; ++j)
-        for (int k = 0; k < nrad; ++k) x[k] = x[k] + chi[((size_t)j * m + i) * nrad + k] * solvent[j].charge;
-      for (int k = 0; k < nrad; ++k) {
-        const double kk = (2 * (k + 1) - 1) * dk / 2;
-        const double v = kk == 0.0 ? 0.0 : 4 * pi * std::exp(-kk * kk / (4 * kG * kG)) / (kk * kk);
-        tab[k] = pd->beta * kEps0Inv * (x[k] * v);
-      }
-      interp_pairs(tab.data(), nrad, pr);
-      std::copy(pr.begin(), pr.end(), s64.begin() + (size_t)i * nrad);
+      std::vector<float2> chi32(chi64.size()), s32(s64.size());
+      for (size_t i = 0; i < chi64.size(); ++i) chi32[i] = make_float2((float)chi64[i].x, (float)chi64[i].y);
+      for (size_t i = 0; i < s64.size(); ++i) s32[i] = make_float2((float)s64[i].x, (float)s64[i].y);
+      c->chi64 = dalloc<double2>(chi64.size());
+      c->chi32 = dalloc<float2>(chi32.size());
+      c->s64 = dalloc<double2>(s64.size());
+      c->s32 = dalloc<float2>(s32.size());
+      CK(cudaMemcpy(c->chi64, chi64.data(), sizeof(double2) * chi64.size(), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(c->chi32, chi32.data(), sizeof(float2) * chi32.size(), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(c->s64, s64.data(), sizeof(double2) * s64.size(), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(c->s32, s32.data(), sizeof(float2) * s32.size(), cudaMemcpyHostToDevice));
     }
-    std::vector<float2> chi32(chi64.size()), s32(s64.size());
-    for (size_t i = 0; i < chi64.size(); ++i) chi32[i] = make_float2((float)chi64[i].x, (float)chi64[i].y);
-    for (size_t i = 0; i < s64.size(); ++i) s32[i] = make_float2((float)s64[i].x, (float)s64[i].y);
-    c->chi64 = dalloc<double2>(chi64.size());
-    c->chi32 = dalloc<float2>(chi32.size());
-    c->s64 = dalloc<double2>(s64.size());
-    c->s32 = dalloc<float2>(s32.size());
-    CK(cudaMemcpy(c->chi64, chi64.data(), sizeof(double2) * chi64.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->chi32, chi32.data(), sizeof(float2) * chi32.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->s64, s64.data(), sizeof(double2) * s64.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->s32, s32.data(), sizeof(float2) * s32.size(), cudaMemcpyHostToDevice));
 
     // sites
     std::vector<SiteP> hv(m);
@@ -1670,21 +1831,12 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
     c->L64 = dalloc<double2>((size_t)G.Nc);
     c->L32 = dalloc<float2>((size_t)G.Nc);
     bind_solute(c, n, solute);
-    (void)h0; (void)h1; (void)h2;
-    c->W = dalloc<double2>((size_t)m * G.Nc);
-    // reduction blocks: about four 16-byte loads per thread, at most 4 per SM
-    c->red_blocks = (int)std::min<long long>(592, std::max<long long>(8, (c->nvec / 4 + 1023) / 1024));
-    c->dpart = dalloc<double>((size_t)c->red_blocks * kVecMax + 64);
-    c->dres = dalloc<double>(4 * kVecMax);
-    const int rows = G.N1 * G.N2;
-    const int rxmin = std::min(std::min(c->tiles[0].RX, c->tiles[1].RX), kStaticRX);
-    c->npart = dalloc<NormPartial>((size_t)((rows + rxmin - 1) / rxmin) * m);
-    c->d_err = dalloc<int>(1);
-    CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    init_work(c);
     // shape-specialised passes (TMA tiles) for the lengths they are built for;
     // RISM3D_GENERIC_PASSES=1 selects the runtime-length passes everywhere
     const char *gen = std::getenv("RISM3D_GENERIC_PASSES");
-    if (static_len_x(G.M) && static_len_yz(G.N1) && static_len_yz(G.N2) && m <= 3 && !(gen && gen[0] == '1')) {
+    if (static_len_x(G.M) && static_len_yz(G.N1) && static_len_yz(G.N2) && m <= 3 && !chi3 &&
+        !(gen && gen[0] == '1')) {
       for (int pr = 0; pr < 2; ++pr) {
         const int B = pr == 0 ? static_B<double>() : static_B<float>();
         const int Bz = pr == 0 ? static_Bz<double>() : static_Bz<float>();
@@ -1693,48 +1845,22 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
         c->stat[pr] = true;
       }
     }
-    // shared-memory opt-in: each kernel may use the device's per-block
-    // opt-in limit minus its own static shared memory
-    int dev = 0, optin = 0;
-    CK(cudaGetDevice(&dev));
-    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    size_t need = 0;
-    for (size_t b : {xsmem<double>(c), ysmem<double>(c), zsmem<double>(c), xsmem<float>(c), ysmem<float>(c),
-                     zsmem<float>(c)})
-      need = std::max(need, b);
-    auto allow = [&](const void *fn) {
-      cudaFuncAttributes fa{};
-      CK(cudaFuncGetAttributes(&fa, fn));
-      const int dyn = optin - (int)fa.sharedSizeBytes;
-      if ((size_t)dyn < need) throw ArgFail{RISM3D_ERR_ARG, "tile exceeds shared memory"};
-      CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
-    };
-    allow((const void *)k_xfwd<double, MODE_F>);
-    allow((const void *)k_xfwd<double, MODE_J>);
-    allow((const void *)k_xfwd<float, MODE_F>);
-    allow((const void *)k_xfwd<float, MODE_J>);
-    allow((const void *)k_xinv<double>);
-    allow((const void *)k_xinv<float>);
-    allow((const void *)k_xfwd<double, MODE_FWD>);  // forward transform of the gradient
-    allow((const void *)k_z<double, MODE_FWD, 16>);
+    size_t need = generic_smem(c);
+    allow_xy(need);
+    auto allow = [&](const void *fn) { allow_smem(fn, need); };
+    allow((const void *)k_z<double, MODE_FWD, 16>);  // forward transform of the gradient
     allow((const void *)k_z<double, MODE_FWD, 8>);
     allow((const void *)k_z<double, MODE_FWD, 4>);
-#define OPTIN_YZ(T)                                  \
-  allow((const void *)k_y<T, false, 16>);            \
-  allow((const void *)k_y<T, true, 16>);             \
-  allow((const void *)k_y<T, false, 8>);             \
-  allow((const void *)k_y<T, true, 8>);              \
-  allow((const void *)k_y<T, false, 4>);             \
-  allow((const void *)k_y<T, true, 4>);              \
+#define OPTIN_Z(T)                                   \
   allow((const void *)k_z<T, MODE_F, 16>);           \
   allow((const void *)k_z<T, MODE_J, 16>);           \
   allow((const void *)k_z<T, MODE_F, 8>);            \
   allow((const void *)k_z<T, MODE_J, 8>);            \
   allow((const void *)k_z<T, MODE_F, 4>);            \
   allow((const void *)k_z<T, MODE_J, 4>);
-    OPTIN_YZ(double)
-    OPTIN_YZ(float)
-#undef OPTIN_YZ
+    OPTIN_Z(double)
+    OPTIN_Z(float)
+#undef OPTIN_Z
     if (c->stat[0]) {
       need = std::max({xs_smem<double, 128>(), ys_smem<double, 256>(), zs_smem<double, 256>(m),
                        xs_smem<float, 128>(), ys_smem<float, 256>(), zs_smem<float, 256>(m)});
@@ -1827,7 +1953,7 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
         for (int a = 0; a < 3; ++a) pc.N[a] = nc[a];
         pc.coarse_h = 0;
         pc.verbosity = 0;
-        create_impl(&pc, m, solvent, n, solute, chi, &c->coarse);
+        create_impl(&pc, m, solvent, n, solute, chi, nullptr, &c->coarse);
         for (int a = 0; a < 3; ++a) {
           const int nf = pd->N[a], ncs = nc[a];
           c->Nc[a] = ncs;
@@ -1888,6 +2014,225 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
   return RISM3D_OK;
 }
 
+// A pure-solvent context (hnc3d_solvent_solve, hnc3d.c:803-1073): the
+// m(m+1)/2 site-site pair fields run through the residual / Jacobian passes
+// with the molecular OZ z pass.  FP64, Newton-GMRES, no preconditioner.
+int solvent_create_impl(const rism3d_problem *pd, int ms, const rism3d_site *solvent, rism3d_ctx **out) {
+  if (!pd || !solvent || !out) throw ArgFail{RISM3D_ERR_ARG, "null argument"};
+  if (ms < 1 || ms > kMaxSolventSites) throw ArgFail{RISM3D_ERR_ARG, "pure-solvent sites must be 1..4"};
+  check_grid(pd);
+  // omega_intra takes k r from L[0] and asserts a cubic box (bgy3d-pure.c:247-250)
+  if (pd->L[1] != pd->L[0] || pd->L[2] != pd->L[0]) throw ArgFail{RISM3D_ERR_ARG, "the pure solvent needs a cubic box"};
+  if (pd->closure == RISM3D_PY) throw ArgFail{RISM3D_ERR_UNSUPPORTED, "PY has no closure differential"};
+  auto c = new rism3d_ctx();
+  try {
+    c->pd = *pd;
+    c->pd.renorm = 0;
+    c->pd.coarse_h = 0;
+    c->pd.precision = RISM3D_FP64;
+    const int np = ms * (ms + 1) / 2;
+    c->pure = ms;
+    c->m = np;
+    c->n = 0;
+    c->solvent.assign(solvent, solvent + ms);
+    init_grid(c, np);
+    const Geo &G = c->g;
+    const double pi = 3.14159265358979323846;
+    std::vector<PairP> hp;
+    for (int i = 0; i < ms; ++i)
+      for (int j = 0; j <= i; ++j) {
+        const rism3d_site &a = solvent[i], &b = solvent[j];
+        const double q2 = a.charge * b.charge;
+        hp.push_back(PairP{0.5 * (a.sigma + b.sigma), std::sqrt(a.epsilon * b.epsilon), q2});
+        const double dx = a.x[0] - b.x[0], dy = a.x[1] - b.x[1], dz = a.x[2] - b.x[2];
+        c->pq2.push_back(q2);
+        c->pwr.push_back(2.0 * pi * std::sqrt(dx * dx + dy * dy + dz * dz) / pd->L[0]);
+      }
+    PairP *dp = dalloc<PairP>(np);
+    CK(cudaMemcpy(dp, hp.data(), sizeof(PairP) * np, cudaMemcpyHostToDevice));
+    c->v64 = dalloc<double>(c->nvec);
+    const double h0 = pd->L[0] / pd->N[0], h1 = pd->L[1] / pd->N[1], h2 = pd->L[2] / pd->N[2];
+    k_pair_field<<<(unsigned)((G.Nr + 255) / 256), 256, 0, c->stream>>>(G, h0, h1, h2, pd->L[0], pd->L[1], pd->L[2],
+                                                                        dp, c->v64);
+    CKL();
+    dfree(dp);
+    c->ck = dalloc<double2>((size_t)np * G.Nc);
+    init_work(c);
+    const size_t need = generic_smem(c);
+    allow_xy(need);
+    allow_smem((const void *)k_z<double, MODE_FWD, 16>, need);
+    allow_smem((const void *)k_z<double, MODE_FWD, 8>, need);
+    allow_smem((const void *)k_z<double, MODE_FWD, 4>, need);
+    switch (ms) {
+      case 1: allow_oz<1>(need); break;
+      case 2: allow_oz<2>(need); break;
+      case 3: allow_oz<3>(need); break;
+      default: allow_oz<4>(need); break;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+  } catch (...) {
+    delete c;
+    throw;
+  }
+  *out = c;
+  return RISM3D_OK;
+}
+
+// The real-space long-range correlation c_L = -beta v_L of every pair by an
+// inverse transform of its k-space form (hnc3d.c:990-1003), into out.
+void long_range_field(rism3d_ctx *c, double *out) {
+  {
+    TimeScope ts(c, TK_Z, 0);
+    switch (c->pure) {
+      case 1: launch_oz_ms<MODE_VL, 1>(c); break;
+      case 2: launch_oz_ms<MODE_VL, 2>(c); break;
+      case 3: launch_oz_ms<MODE_VL, 3>(c); break;
+      default: launch_oz_ms<MODE_VL, 4>(c); break;
+    }
+  }
+  launch_y<double, true>(c);
+  TimeScope ts(c, TK_XINV, 0);
+  const int RX = c->tl<double>().RX;
+  dim3 gx((c->g.N1 * c->g.N2 + RX - 1) / RX, c->m);
+  k_xinv<double><<<gx, 256, xsmem<double>(c), c->stream>>>(c->g, c->plan<double>(0), RX, c->work<double>(), out, out,
+                                                          1.0 / (double)c->g.Nr, 0.0, postw<double>(c), c->npart);
+  CKL();
+}
+
+// Tabulates the 1D RISM t(r) of the pure solvent on the upscaled radial grid
+// (rmax = 2 max(L), nrad = 16 max(N): upscale, hnc3d.c:776-787) on the 3D
+// grid as the initial guess (hnc3d.c:824-851).
+void solvent_guess(rism3d_ctx *c, double *T) {
+  const rism3d_problem &pd = c->pd;
+  const int ms = c->pure;
+  rism3d_problem up = pd;
+  up.rmax = 4 * std::max(std::max(pd.L[0], pd.L[1]), pd.L[2]) / 2;
+  up.nrad = 16 * std::max(std::max(pd.N[0], pd.N[1]), pd.N[2]);
+  up.norm_tol = std::max(pd.norm_tol, 1e-10);
+  const int nrad = up.nrad;
+  std::vector<double> chi((size_t)ms * ms * nrad), t((size_t)ms * ms * nrad, 0.0);
+  const int rc = rism1d_solvent_chi(&up, 0.0, ms, c->solvent.data(), chi.data(), t.data(), nullptr);
+  if (rc != RISM3D_OK) throw CudaFail{rc};
+  std::vector<double2> tab, pr;
+  for (int i = 0; i < ms; ++i)
+    for (int j = 0; j <= i; ++j) {
+      interp_pairs(t.data() + ((size_t)i * ms + j) * nrad, nrad, pr);
+      tab.insert(tab.end(), pr.begin(), pr.end());
+    }
+  double2 *dt = dalloc<double2>(tab.size());
+  CK(cudaMemcpy(dt, tab.data(), sizeof(double2) * tab.size(), cudaMemcpyHostToDevice));
+  const Geo &G = c->g;
+  const double h0 = pd.L[0] / pd.N[0], h1 = pd.L[1] / pd.N[1], h2 = pd.L[2] / pd.N[2];
+  k_rtab<<<(unsigned)((G.Nr + 255) / 256), 256, 0, c->stream>>>(G, h0, h1, h2, pd.L[0], pd.L[1], pd.L[2], dt, nrad,
+                                                                up.rmax / nrad, T);
+  CKL();
+  dfree(dt);
+}
+
+template <int MS> void chi_out_launch(rism3d_ctx *c, double2 *out) {
+  PureParams<MS> pp{};
+  pp.rho = c->pd.rho;
+  pp.beta = c->pd.beta;
+  pp.h3 = c->h3;
+  for (int p = 0; p < PureParams<MS>::NP; ++p) {
+    pp.q2[p] = c->pq2[p];
+    pp.wr[p] = c->pwr[p];
+  }
+  k_chi_out<MS><<<vec_grid((long long)c->g.Nh * c->g.N1 * c->g.N2), 256, 0, c->stream>>>(c->g, c->work<double>(),
+                                                                                           pp, out);
+  CKL();
+}
+
+// Newton-GMRES on the pair fields from T (device, in/out), then the
+// observables, chi - 1 on the k grid and g (host outputs, each optional).
+int solvent_solve_impl(rism3d_ctx *c, double *T, double *chi_out, double *g_out, rism3d_solvent_result *res) {
+  const rism3d_problem &pd = c->pd;
+  *res = rism3d_solvent_result{};
+  c->f_evals = c->jv_evals = 0;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, c->stream));
+  const int restart = pd.krylov_restart > 0 ? std::min(pd.krylov_restart, 200) : 30;
+  NewtonOut o = newton<double, double>(c, T, pd.norm_tol, pd.max_iter, 1e-3, restart);
+  const Geo &G = c->g;
+  const long long nv = c->nvec;
+  double *cl = dalloc<double>(nv), *h = dalloc<double>(nv);
+  double *g = g_out ? dalloc<double>(nv) : nullptr;
+  long_range_field(c, cl);
+  const int rb = (int)std::min<long long>(2 * 148, (G.Nr + 255) / 256);
+  double *part = dalloc<double>((size_t)rb * 5);
+  k_solvent_obs<<<rb, 256, 0, c->stream>>>(G, c->pure, T, c->v64, cl, pd.beta, pd.closure, h, g, part);
+  CKL();
+  std::vector<double> hp((size_t)rb * 5);
+  CK(cudaMemcpyAsync(hp.data(), part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, c->stream));
+  if (chi_out) {
+    fwd3d(c, h);
+    const long long nk = (long long)G.Nh * G.N1 * G.N2;
+    double2 *dchi = dalloc<double2>((size_t)c->m * nk);
+    switch (c->pure) {
+      case 1: chi_out_launch<1>(c, dchi); break;
+      case 2: chi_out_launch<2>(c, dchi); break;
+      case 3: chi_out_launch<3>(c, dchi); break;
+      default: chi_out_launch<4>(c, dchi); break;
+    }
+    CK(cudaMemcpyAsync(chi_out, dchi, sizeof(double2) * (size_t)c->m * nk, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    dfree(dchi);
+  }
+  if (g_out) CK(cudaMemcpyAsync(g_out, g, sizeof(double) * nv, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaEventRecord(e1, c->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  dfree(cl);
+  dfree(h);
+  dfree(g);
+  dfree(part);
+  double a[5] = {0, 0, 0, 0, 0};
+  for (int b = 0; b < rb; ++b)
+    for (int k = 0; k < 5; ++k) a[k] += hp[(size_t)b * 5 + k];
+  // mu = rho h^3 sum / beta (chempot, hnc3d.c:604-623); kappa and a from
+  // rho c(k=0) = rho h^3 sum c (print_kappa, hnc3d.c:738-760)
+  const double f = pd.rho * c->h3 / pd.beta;
+  res->mu = a[0] * f;
+  res->mu_hnc = a[1] * f;
+  res->mu_kh = a[2] * f;
+  res->mu_gf = a[3] * f;
+  const double c0 = a[4] * (pd.rho * c->h3);
+  res->a = c0 / 2 / pd.beta;
+  res->kappa = pd.beta / (1 - c0) / pd.rho;
+  res->resid_inf = o.rinf;
+  res->resid_2 = o.r2;
+  res->newton_iters = o.iters;
+  res->f_evals = c->f_evals;
+  res->jv_evals = c->jv_evals;
+  res->seconds = ms * 1e-3;
+  res->status = o.nan ? RISM3D_ERR_NAN : (o.converged ? RISM3D_OK : RISM3D_ERR_NOT_CONVERGED);
+  return res->status;
+}
+
+// One solve on a fresh context from host buffers (rism3d_solute_solve).
+int solve_on(rism3d_ctx *ctx, double *t_inout, double *g_out, rism3d_result *out) {
+  const size_t bytes = sizeof(double) * ctx->nvec;
+  double *T = dalloc<double>(ctx->nvec);
+  double *g = g_out ? dalloc<double>(ctx->nvec) : nullptr;
+  struct Free { double *a, *b; ~Free() { dfree(a); dfree(b); } } fr{T, g};
+  if (t_inout) CK(cudaMemcpy(T, t_inout, bytes, cudaMemcpyHostToDevice));
+  else CK(cudaMemset(T, 0, bytes));
+  rism3d_result r{};
+  int st = solve_impl(ctx, T, &r);
+  observables_impl(ctx, T, g, &r);
+  r.launches += 2;  // the observables' kernels
+  r.status = st;
+  if (t_inout) CK(cudaMemcpy(t_inout, T, bytes, cudaMemcpyDeviceToHost));
+  if (g_out) CK(cudaMemcpy(g_out, g, bytes, cudaMemcpyDeviceToHost));
+  if (out) *out = r;
+  return st;
+}
+
 template <typename F> int guard(F &&f) {
   try {
     return f();
@@ -1936,7 +2281,7 @@ const char *rism3d_last_error(void) { return g_last_error.c_str(); }
 int rism3d_ctx_create(const rism3d_problem *pd, int m, const rism3d_site *solvent, int n,
                       const rism3d_site *solute, const double *chi, rism3d_ctx **ctx) {
   if (ctx) *ctx = nullptr;
-  return guard([&] { return create_impl(pd, m, solvent, n, solute, chi, ctx); });
+  return guard([&] { return create_impl(pd, m, solvent, n, solute, chi, nullptr, ctx); });
 }
 
 void rism3d_ctx_destroy(rism3d_ctx *ctx) { delete ctx; }
@@ -1958,6 +2303,7 @@ int rism3d_jacobian_t1(rism3d_ctx *ctx, const double *T, const double *dT, doubl
   if (ctx->pd.closure == RISM3D_PY) return RISM3D_ERR_UNSUPPORTED;
   return guard([&] {
     double *d = slopebuf<double>(ctx);
+    if (ctx->pure) eval_F<double>(ctx, T, JdT, nullptr);  // C(k) at T for the OZ differential
     closure_slope<double, double>(ctx, T, d);
     eval_J<double>(ctx, d, dT, 1.0, JdT, nullptr);
     CK(cudaStreamSynchronize(ctx->stream));
@@ -1967,6 +2313,7 @@ int rism3d_jacobian_t1(rism3d_ctx *ctx, const double *T, const double *dT, doubl
 
 int rism3d_iterate_t1_f32(rism3d_ctx *ctx, const float *T, float *dT, double *resid) {
   if (!ctx || !T || !dT) return RISM3D_ERR_ARG;
+  if (ctx->pure) return RISM3D_ERR_UNSUPPORTED;
   return guard([&] {
     double r[2];
     eval_F<float>(ctx, T, dT, r);
@@ -1976,6 +2323,7 @@ int rism3d_iterate_t1_f32(rism3d_ctx *ctx, const float *T, float *dT, double *re
 }
 
 int rism3d_jacobian_t1_f32(rism3d_ctx *ctx, const float *T, const float *dT, float *JdT) {
+  if (ctx && ctx->pure) return RISM3D_ERR_UNSUPPORTED;
   if (!ctx || !T || !dT || !JdT) return RISM3D_ERR_ARG;
   if (ctx->pd.closure == RISM3D_PY) return RISM3D_ERR_UNSUPPORTED;
   return guard([&] {
@@ -1989,11 +2337,13 @@ int rism3d_jacobian_t1_f32(rism3d_ctx *ctx, const float *T, const float *dT, flo
 
 int rism3d_solve(rism3d_ctx *ctx, double *T, rism3d_result *out) {
   if (!ctx || !T) return RISM3D_ERR_ARG;
+  if (ctx->pure) return RISM3D_ERR_UNSUPPORTED;
   return guard([&] { return solve_impl(ctx, T, out); });
 }
 
 int rism3d_observables(rism3d_ctx *ctx, const double *T, double *g, rism3d_result *out) {
   if (!ctx || !T) return RISM3D_ERR_ARG;
+  if (ctx->pure) return RISM3D_ERR_UNSUPPORTED;
   return guard([&] { return observables_impl(ctx, T, g, out); });
 }
 
@@ -2025,25 +2375,59 @@ int rism3d_solute_solve(const rism3d_problem *pd, int m, const rism3d_site *solv
     if (out) { std::memset(out, 0, sizeof(*out)); out->status = rc; }
     return rc;
   }
-  rc = guard([&] {
-    const size_t bytes = sizeof(double) * ctx->nvec;
-    double *T = dalloc<double>(ctx->nvec);
-    double *g = g_out ? dalloc<double>(ctx->nvec) : nullptr;
-    struct Free { double *a, *b; ~Free() { dfree(a); dfree(b); } } fr{T, g};
-    if (t_inout) CK(cudaMemcpy(T, t_inout, bytes, cudaMemcpyHostToDevice));
-    else CK(cudaMemset(T, 0, bytes));
-    rism3d_result r{};
-    int st = solve_impl(ctx, T, &r);
-    observables_impl(ctx, T, g, &r);
-    r.launches += 2;  // the observables' kernels
-    r.status = st;
-    if (t_inout) CK(cudaMemcpy(t_inout, T, bytes, cudaMemcpyDeviceToHost));
-    if (g_out) CK(cudaMemcpy(g_out, g, bytes, cudaMemcpyDeviceToHost));
-    if (out) *out = r;
-    return st;
-  });
+  rc = guard([&] { return solve_on(ctx, t_inout, g_out, out); });
   rism3d_ctx_destroy(ctx);
   if (out && rc < 0 && out->status == 0) out->status = rc;
+  return rc;
+}
+
+int rism3d_ctx_create_chi3(const rism3d_problem *pd, int m, const rism3d_site *solvent, int n,
+                           const rism3d_site *solute, const double *chi3, rism3d_ctx **ctx) {
+  if (ctx) *ctx = nullptr;
+  if (!chi3) return RISM3D_ERR_ARG;
+  return guard([&] { return create_impl(pd, m, solvent, n, solute, nullptr, chi3, ctx); });
+}
+
+int rism3d_solute_solve_chi3(const rism3d_problem *pd, int m, const rism3d_site *solvent, int n,
+                             const rism3d_site *solute, const double *chi3, double *t_inout, double *g_out,
+                             rism3d_result *out) {
+  rism3d_ctx *ctx = nullptr;
+  int rc = rism3d_ctx_create_chi3(pd, m, solvent, n, solute, chi3, &ctx);
+  if (rc != RISM3D_OK) {
+    if (out) { std::memset(out, 0, sizeof(*out)); out->status = rc; }
+    return rc;
+  }
+  rc = guard([&] { return solve_on(ctx, t_inout, g_out, out); });
+  rism3d_ctx_destroy(ctx);
+  if (out && rc < 0 && out->status == 0) out->status = rc;
+  return rc;
+}
+
+int rism3d_solvent_ctx_create(const rism3d_problem *pd, int m, const rism3d_site *solvent, rism3d_ctx **ctx) {
+  if (ctx) *ctx = nullptr;
+  return guard([&] { return solvent_create_impl(pd, m, solvent, ctx); });
+}
+
+int rism3d_solvent_solve(const rism3d_problem *pd, int m, const rism3d_site *solvent, const double *t_in,
+                         double *t_out, double *chi_out, double *g_out, rism3d_solvent_result *out) {
+  rism3d_solvent_result res{};
+  rism3d_ctx *ctx = nullptr;
+  int rc = rism3d_solvent_ctx_create(pd, m, solvent, &ctx);
+  if (rc == RISM3D_OK) {
+    rc = guard([&] {
+      const size_t bytes = sizeof(double) * ctx->nvec;
+      double *T = dalloc<double>(ctx->nvec);
+      struct Free { double *a; ~Free() { dfree(a); } } fr{T};
+      if (t_in) CK(cudaMemcpy(T, t_in, bytes, cudaMemcpyHostToDevice));
+      else solvent_guess(ctx, T);
+      const int st = solvent_solve_impl(ctx, T, chi_out, g_out, &res);
+      if (t_out) CK(cudaMemcpy(t_out, T, bytes, cudaMemcpyDeviceToHost));
+      return st;
+    });
+    rism3d_ctx_destroy(ctx);
+  }
+  if (res.status == 0) res.status = rc;
+  if (out) *out = res;
   return rc;
 }
 
@@ -2084,6 +2468,7 @@ int rism3d_solve_batch(int m, const rism3d_site *solvent, int njobs, rism3d_job 
 
 int rism3d_ctx_set_solute(rism3d_ctx *ctx, int n, const rism3d_site *solute) {
   if (!ctx || n < 0 || (n > 0 && !solute)) return RISM3D_ERR_ARG;
+  if (ctx->pure) return RISM3D_ERR_UNSUPPORTED;
   return guard([&] {
     bind_solute(ctx, n, solute);
     return (int)RISM3D_OK;
@@ -2092,16 +2477,19 @@ int rism3d_ctx_set_solute(rism3d_ctx *ctx, int n, const rism3d_site *solute) {
 
 int rism3d_jacobian_transpose_t1(rism3d_ctx *ctx, const double *T, const double *dT, double *JT) {
   if (!ctx || !T || !dT || !JT) return RISM3D_ERR_ARG;
+  if (ctx->pure) return RISM3D_ERR_UNSUPPORTED;
   return guard([&] { return jacobian_transpose_impl(ctx, T, dT, JT); });
 }
 
 int rism3d_gradient(rism3d_ctx *ctx, const double *T, rism3d_grad *grad) {
   if (!ctx || !T || !grad) return RISM3D_ERR_ARG;
+  if (ctx->pure) return RISM3D_ERR_UNSUPPORTED;
   return guard([&] { return gradient_impl(ctx, T, grad); });
 }
 
 int rism3d_response(rism3d_ctx *ctx, const double *T, rism3d_grad *grad) {
   if (!ctx || !T || !grad) return RISM3D_ERR_ARG;
+  if (ctx->pure) return RISM3D_ERR_UNSUPPORTED;
   return guard([&] { return response_impl(ctx, T, grad); });
 }
 

@@ -115,20 +115,41 @@ def rism_solvent(solvent, settings):
     return {"susceptibility": chi, "t": t, "free-energy": mu.value}
 
 
+def npairs(m):
+    return m * (m + 1) // 2
+
+
+def _chi_arg(chi, m, pd):
+    """(is_3d, contiguous array): a radial [m][m][nrad] susceptibility, or
+    chi - 1 on the k grid [m(m+1)/2][N2][N1][N0/2+1] complex (the
+    --solvent-3d kernel of hnc3d_run_solvent)."""
+    if np.iscomplexobj(chi):
+        c3 = np.ascontiguousarray(chi, dtype=np.complex128)
+        want = (npairs(m), pd.N[2], pd.N[1], pd.N[0] // 2 + 1)
+        if c3.shape != want:
+            raise ValueError(f"3D chi must be {list(want)}, got {c3.shape}")
+        return True, c3
+    c = np.ascontiguousarray(chi, dtype=np.float64)
+    if c.shape != (m, m, pd.nrad):
+        raise ValueError(f"chi must be [{m}][{m}][{pd.nrad}], got {c.shape}")
+    return False, c
+
+
 def hnc3d_run_solute(solute, solvent, settings, chi, restart=None, want_g=True, want_restart=True):
     """One 3D-RISM solute solve with host buffers (rism3d_solute_solve).
 
     chi: [m][m][nrad] solvent susceptibility (not offset by one) on the
     radial k-grid (p + 1/2) pi / rmax; settings must then carry the rmax and
-    nrad it was computed with.  restart: initial t [m][N2][N1][N0] or None.
-    With restart None and want_restart False no t crosses the host link.
+    nrad it was computed with.  Or chi - 1 on the 3D k grid as returned by
+    hnc3d_run_solvent (complex), the reference's --solvent-3d: then the
+    solve takes the no-renorm form (rism3d_solute_solve_chi3).
+    restart: initial t [m][N2][N1][N0] or None.  With restart None and
+    want_restart False no t crosses the host link.
     """
     L = _abi.lib()
     pd = problem_data(settings)
     m, n = len(solvent), len(solute)
-    chi = np.ascontiguousarray(chi, dtype=np.float64)
-    if chi.shape != (m, m, pd.nrad):
-        raise ValueError(f"chi must be [{m}][{m}][{pd.nrad}], got {chi.shape}")
+    is3d, chi = _chi_arg(chi, m, pd)
     shape = (m, pd.N[2], pd.N[1], pd.N[0])
     if restart is None and not want_restart:
         t = None
@@ -138,9 +159,9 @@ def hnc3d_run_solute(solute, solvent, settings, chi, restart=None, want_g=True, 
             raise ValueError("restart has the wrong shape")
     g = np.empty(shape) if want_g else None
     res = _abi.Result()
-    rc = L.rism3d_solute_solve(ctypes.byref(pd), m, _sites(solvent), n, _sites(solute), _dptr(chi),
-                               _dptr(t) if t is not None else None, _dptr(g) if g is not None else None,
-                               ctypes.byref(res))
+    fn = L.rism3d_solute_solve_chi3 if is3d else L.rism3d_solute_solve
+    rc = fn(ctypes.byref(pd), m, _sites(solvent), n, _sites(solute), _dptr(chi),
+            _dptr(t) if t is not None else None, _dptr(g) if g is not None else None, ctypes.byref(res))
     out = _result_dict(res)
     if rc != _abi.OK and rc != _abi.ERR_NOT_CONVERGED:
         raise _abi.RismError(rc, "hnc3d_run_solute")
@@ -149,6 +170,43 @@ def hnc3d_run_solute(solute, solvent, settings, chi, restart=None, want_g=True, 
     out["GUV"] = g
     out["RESTART"] = t
     return out
+
+
+def hnc3d_run_solvent(solvent, settings, restart=None, want_g=True, want_restart=True):
+    """3D RISM of the pure solvent (rism3d_solvent_solve), mirroring the
+    Scheme ``hnc3d-run-solvent`` (guile/bgy3d.scm:378-384) and its C body
+    hnc3d_solvent_solve (hnc3d.c:803-1073).  Where the reference writes
+    chi - 1 to x%d%d-fft.bin and g to g%d%d.bin, this returns them:
+
+      "susceptibility-3d": chi - 1 on the k grid, complex
+          [m(m+1)/2][N2][N1][N0/2+1] (pair p = i(i+1)/2 + j, i >= j) -- the
+          chi argument of hnc3d_run_solute for the --solvent-3d solve;
+      "GVV": g [m(m+1)/2][N2][N1][N0]; "RESTART": t;
+      "free-energy" (the closure's functional), "free-energy-all" {HNC, KH,
+      GF}, "compressibility", "a" (print_kappa), solver counters.
+    restart: initial pair fields, or None for the 1D RISM guess."""
+    L = _abi.lib()
+    pd = problem_data(settings)
+    m = len(solvent)
+    shape = (npairs(m), pd.N[2], pd.N[1], pd.N[0])
+    t_in = None if restart is None else np.ascontiguousarray(restart, dtype=np.float64)
+    if t_in is not None and t_in.shape != shape:
+        raise ValueError("restart has the wrong shape")
+    t_out = np.empty(shape) if want_restart else None
+    g = np.empty(shape) if want_g else None
+    chi3 = np.empty((npairs(m), pd.N[2], pd.N[1], pd.N[0] // 2 + 1), dtype=np.complex128)
+    res = _abi.SolventResult()
+    rc = L.rism3d_solvent_solve(ctypes.byref(pd), m, _sites(solvent),
+                                _dptr(t_in) if t_in is not None else None,
+                                _dptr(t_out) if t_out is not None else None, _dptr(chi3),
+                                _dptr(g) if g is not None else None, ctypes.byref(res))
+    if rc != _abi.OK:
+        raise _abi.RismError(rc, "hnc3d_run_solvent")
+    return {"free-energy": res.mu, "free-energy-all": {"HNC": res.mu_hnc, "KH": res.mu_kh, "GF": res.mu_gf},
+            "compressibility": res.kappa, "a": res.a, "resid-inf": res.resid_inf, "resid-2": res.resid_2,
+            "status": res.status, "newton-iters": res.newton_iters, "f-evals": res.f_evals,
+            "jv-evals": res.jv_evals, "seconds": res.seconds, "susceptibility-3d": chi3, "GVV": g,
+            "RESTART": t_out}
 
 
 def _grad_struct(n):
@@ -242,20 +300,30 @@ class RismContext:
     """Device-resident problem (rism3d_ctx) on the current CUDA device."""
 
     def __init__(self, solute, solvent, settings, chi):
+        """chi: the radial susceptibility, or chi - 1 on the 3D k grid
+        (complex, from hnc3d_run_solvent; the --solvent-3d kernel).  With
+        solute None the context is the pure solvent's (rism3d_solvent_ctx_
+        create): its vectors are the m(m+1)/2 pair fields and iterate_t1 /
+        jacobian_t1 evaluate iterate_t2 and its Jacobian; chi is unused."""
         import torch  # device memory only
         self._torch = torch
         L = _abi.lib()
         self.pd = problem_data(settings)
-        self.m, self.n = len(solvent), len(solute)
-        chi = np.ascontiguousarray(chi, dtype=np.float64)
-        if chi.shape != (self.m, self.m, self.pd.nrad):
-            raise ValueError("chi has the wrong shape")
-        self._chi = chi
         h = ctypes.c_void_p()
-        _abi.check(L.rism3d_ctx_create(ctypes.byref(self.pd), self.m, _sites(solvent), self.n,
-                                       _sites(solute), _dptr(chi), ctypes.byref(h)), "rism3d_ctx_create")
+        if solute is None:
+            self.m, self.n = len(solvent), 0
+            _abi.check(L.rism3d_solvent_ctx_create(ctypes.byref(self.pd), self.m, _sites(solvent), ctypes.byref(h)),
+                       "rism3d_solvent_ctx_create")
+            self.shape = (npairs(self.m), self.pd.N[2], self.pd.N[1], self.pd.N[0])
+        else:
+            self.m, self.n = len(solvent), len(solute)
+            is3d, chi = _chi_arg(chi, self.m, self.pd)
+            self._chi = chi
+            fn = L.rism3d_ctx_create_chi3 if is3d else L.rism3d_ctx_create
+            _abi.check(fn(ctypes.byref(self.pd), self.m, _sites(solvent), self.n, _sites(solute), _dptr(chi),
+                          ctypes.byref(h)), "rism3d_ctx_create")
+            self.shape = (self.m, self.pd.N[2], self.pd.N[1], self.pd.N[0])
         self._h = h
-        self.shape = (self.m, self.pd.N[2], self.pd.N[1], self.pd.N[0])
         self.size = int(L.rism3d_ctx_size(h))
 
     def close(self):

@@ -319,6 +319,62 @@ int rism3d_profile(rism3d_ctx *ctx, int on, double *ms, long long *launches);
 int rism3d_jacobian_apply_noalloc(const rism3d_problem *pd, int m, const double *chi,
                                   const double *d, const double *dT, double *JdT);
 
+/* ---- 3D solvent susceptibility (the --solvent-3d path) ---------------- */
+
+/* Results of the pure-solvent solve. */
+typedef struct rism3d_solvent_result {
+  double mu;          /* excess chemical potential, the closure's functional, kcal/mol */
+  double mu_hnc, mu_kh, mu_gf; /* the HNC, KH and GF functionals (print_chempot, hnc3d.c:674-694) */
+  double a;           /* rho c(k=0) / 2 beta, kcal/mol (print_kappa, hnc3d.c:738-760) */
+  double kappa;       /* isothermal compressibility beta / (rho (1 - rho c(k=0))), A^3/kcal */
+  double resid_inf, resid_2;
+  int status, newton_iters, f_evals, jv_evals;
+  double seconds;     /* device time of the solve and post-processing */
+} rism3d_solvent_result;
+
+/*
+  3D RISM of the pure solvent: replaces hnc3d_solvent_solve (hnc3d.c:
+  803-1073).  The unknowns are the m(m+1)/2 site-site indirect correlations
+  t_ij, i >= j, packed as pair p = i(i+1)/2 + j (vec_aliases_create2,
+  bgy3d-vec.h:739-758), each a field [N2][N1][N0] centred on the box; the
+  per-k molecular OZ equation h = (1 - rho W C)^-1 W C W with the
+  intramolecular W = sinc(k r_ij) and the site-site potentials of
+  bgy3d_pair_potential (bgy3d-force.c:123-147).  Newton-GMRES with the OZ
+  equation's exact Jacobian (the reference differences F instead).  Uses
+  pd->N, L (a cubic box), beta, rho, closure (not PY), norm_tol, max_iter,
+  krylov_restart, ew_forcing; m <= 4.
+    t_in     host [m(m+1)/2][N2][N1][N0] initial guess, or NULL for the 1D
+             RISM t(r) on the upscaled radial grid (rmax = 2 max(L), nrad =
+             16 max(N); hnc3d.c:776-851);
+    t_out    host, the converged pair fields, or NULL;
+    chi_out  host complex [m(m+1)/2][N2][N1][N0/2+1] (re, im pairs), or NULL:
+             chi - 1 = rho h(k) + omega - 1 at the grid corner, the content of
+             the reference's x%d%d-fft.bin (hnc3d.c:1011-1047), as the chi3
+             input of rism3d_solute_solve_chi3;
+    g_out    host [m(m+1)/2][N2][N1][N0] g = 1 + h, or NULL. */
+int rism3d_solvent_solve(const rism3d_problem *pd, int m, const rism3d_site *solvent,
+                         const double *t_in, double *t_out, double *chi_out, double *g_out,
+                         rism3d_solvent_result *out);
+
+/* A context on the pure solvent's pair fields: rism3d_iterate_t1 /
+   rism3d_jacobian_t1 then evaluate iterate_t2 (hnc3d.c:353-456) and its
+   Jacobian (FP64); the solute-only entry points return
+   RISM3D_ERR_UNSUPPORTED. */
+int rism3d_solvent_ctx_create(const rism3d_problem *pd, int m, const rism3d_site *solvent,
+                              rism3d_ctx **ctx);
+
+/* The solute solve on a 3D solvent kernel: chi3 = chi - 1 on the k grid
+   (host complex [m(m+1)/2][N2][N1][N0/2+1], as rism3d_solvent_solve writes
+   it) replaces the radial chi table -- the `solvent-3d` branch of
+   solvent_kernel (hnc3d.c:1575-1587), which also selects the no-renorm
+   long-range form.  Other arguments as rism3d_solute_solve; pd->rmax,
+   nrad, renorm and coarse_h are ignored (no two-grid preconditioner). */
+int rism3d_ctx_create_chi3(const rism3d_problem *pd, int m, const rism3d_site *solvent,
+                           int n, const rism3d_site *solute, const double *chi3, rism3d_ctx **ctx);
+int rism3d_solute_solve_chi3(const rism3d_problem *pd, int m, const rism3d_site *solvent,
+                             int n, const rism3d_site *solute, const double *chi3,
+                             double *t_inout, double *g_out, rism3d_result *out);
+
 /* ---- solvent susceptibility (setup, CPU) ------------------------------ */
 
 /* 1D RISM / DRISM of the pure solvent: replaces rism_solvent()

@@ -126,3 +126,32 @@ def test_response_is_the_derivative_when_uncharged(fixture_loader):
         mu.append(solve(moved, out["T"])["mu"])
     fd = (mu[0] - mu[1]) / (2 * h)
     assert abs(dE[0, 0] - fd) < 1e-6 * max(1.0, abs(fd))
+
+
+@pytest.fixture(scope="module")
+def solvent3d_water():
+    """The 3D pure-solvent run of test/Makefile:19-31 (water, KH, 96^3, L 10)."""
+    from oracle import solvent3d
+    w = find_molecule("water")
+    return w, solvent3d.solvent_solve((96,) * 3, (20.0,) * 3, 1.6889, 0.033427745, cl.KH, w, tol=1e-12)
+
+
+def test_3d_solvent_water_golden(solvent3d_water):
+    """test/out/water.hnc3d.g2: mu = -4.161039 (HNC), -5.793348 (KH), -9.595354 (GF)."""
+    _, out = solvent3d_water
+    mu = out["mu_all"]
+    assert abs(mu["HNC"] - -4.161039) < 5e-7
+    assert abs(mu["KH"] - -5.793348) < 5e-7
+    assert abs(mu["GF"] - -9.595354) < 5e-7
+
+
+def test_3d_solvent_water_solute_golden(solvent3d_water):
+    """test/out/water.hnc3d.g1: the water solute on the 3D solvent's chi
+    (--solvent-3d): mu = -2.284209 (HNC), -3.894980 (KH), -5.870259 (GF)."""
+    w, out = solvent3d_water
+    res = hnc3d.solute_solve((96,) * 3, (20.0,) * 3, 1.6889, 0.033427745, cl.KH, w, w, None, None,
+                             chi3=out["chi_fft"], tol=1e-12)
+    mu = res["mu_all"]
+    assert abs(mu["HNC"] - -2.284209) < 5e-7
+    assert abs(mu["KH"] - -3.894980) < 5e-7
+    assert abs(mu["GF"] - -5.870259) < 5e-7
