@@ -75,6 +75,16 @@ class SolventResult(ctypes.Structure):
                 ("seconds", ctypes.c_double)]
 
 
+D3 = ctypes.c_double * 3
+D33 = (ctypes.c_double * 3) * 3
+
+
+class InfoResult(ctypes.Structure):
+    _fields_ = [("q_u", ctypes.c_double), ("d_u", D3), ("Q_u", D33), ("q_v", ctypes.c_double), ("d_v", D3),
+                ("Q_v", D33), ("d_n", D3), ("U_v_rho_N", ctypes.c_double), ("U_v_rho_N_trilinear", ctypes.c_double),
+                ("U_v_rho_u", ctypes.c_double), ("rho_v_U_u", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+
 # Every entry point declared in include/rism3d.h (checked by the CPU tests).
 EXPORTS = [
     "rism3d_problem_defaults", "rism3d_solute_solve", "rism3d_ctx_create",
@@ -85,7 +95,7 @@ EXPORTS = [
     "rism3d_precondition", "rism3d_coarse_grid", "rism3d_solve_batch",
     "rism3d_solute_grad", "rism3d_gradient", "rism3d_jacobian_transpose_t1", "rism3d_ctx_set_solute",
     "rism3d_response", "rism3d_solvent_solve", "rism3d_solvent_ctx_create", "rism3d_ctx_create_chi3",
-    "rism3d_solute_solve_chi3",
+    "rism3d_solute_solve_chi3", "rism3d_info", "rism3d_moments",
 ]
 
 _lib = None
@@ -154,6 +164,10 @@ def lib():
     L.rism3d_ctx_create_chi3.restype = I
     L.rism3d_solute_solve_chi3.argtypes = [P(Problem), I, P(Site), I, P(Site), P(D), P(D), P(D), P(Result)]
     L.rism3d_solute_solve_chi3.restype = I
+    L.rism3d_info.argtypes = [V, V, P(InfoResult), P(D)]
+    L.rism3d_info.restype = I
+    L.rism3d_moments.argtypes = [V, V, I, P(D)]
+    L.rism3d_moments.restype = I
     _lib = L
     return L
 

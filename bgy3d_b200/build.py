@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librism3d.so")
 SOURCES = ["rism3d.cu", "rism1d.cpp", "noalloc.cu"]
 HEADERS = ["fft_core.cuh", "kernels.cuh", "fft_static.cuh", "kernels_static.cuh", "krylov.cuh", "twogrid.cuh",
-           "twogrid_fft.cuh", "grad.cuh", "solvent.cuh"]
+           "twogrid_fft.cuh", "grad.cuh", "solvent.cuh", "info.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 

@@ -27,6 +27,7 @@
 #include "kernels_static.cuh"
 #include "grad.cuh"
 #include "krylov.cuh"
+#include "info.cuh"
 #include "rism3d.h"
 #include "solvent.cuh"
 #include "twogrid.cuh"
@@ -2214,6 +2215,144 @@ int solvent_solve_impl(rism3d_ctx *c, double *T, double *chi_out, double *g_out,
   return res->status;
 }
 
+// Moments of shift + scale * v over `nf` fields into out[nf][13] (q, d[3],
+// Q[3][3]) with the h^3, h_a, h_a h_b scales of bgy3d_moments.
+void moments_of(rism3d_ctx *c, const double *v, int nf, double shift, double scale, double *out) {
+  const Geo &G = c->g;
+  const int rb = (int)std::min<long long>(2 * 148, (G.Nr + 255) / 256);
+  double *part = dalloc<double>((size_t)rb * nf * 10);
+  k_moments<<<dim3(rb, nf), 256, 0, c->stream>>>(G, v, nf, shift, scale, part);
+  CKL();
+  std::vector<double> hp((size_t)rb * nf * 10);
+  CK(cudaMemcpyAsync(hp.data(), part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  dfree(part);
+  const double h[3] = {c->pd.L[0] / c->pd.N[0], c->pd.L[1] / c->pd.N[1], c->pd.L[2] / c->pd.N[2]};
+  const double dV = c->h3;
+  for (int f = 0; f < nf; ++f) {
+    double a[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int b = 0; b < rb; ++b)
+      for (int k = 0; k < 10; ++k) a[k] += hp[((size_t)f * rb + b) * 10 + k];
+    double *o = out + (size_t)f * 13;
+    o[0] = dV * a[0];
+    for (int d = 0; d < 3; ++d) o[1 + d] = dV * h[d] * a[1 + d];
+    const int diag[3] = {4, 5, 6};
+    for (int d = 0; d < 3; ++d) o[4 + 4 * d] = dV * h[d] * h[d] * a[diag[d]];
+    o[4 + 1] = o[4 + 3] = dV * h[0] * h[1] * a[7];
+    o[4 + 5] = o[4 + 7] = dV * h[1] * h[2] * a[8];
+    o[4 + 2] = o[4 + 6] = dV * h[0] * h[2] * a[9];
+  }
+}
+
+int info_impl(rism3d_ctx *c, const double *T, rism3d_info_result *res, double *site_potential) {
+  const rism3d_problem &pd = c->pd;
+  const Geo &G = c->g;
+  *res = rism3d_info_result{};
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, c->stream));
+  const double h[3] = {pd.L[0] / pd.N[0], pd.L[1] / pd.N[1], pd.L[2] / pd.N[2]};
+  const unsigned nb = (unsigned)((G.Nr + 255) / 256);
+  double *A = dalloc<double>(c->nvec), *ru = dalloc<double>(G.Nr), *uc = dalloc<double>(G.Nr);
+  double2 *Rv = dalloc<double2>((size_t)G.Nc);
+  CK(cudaMemsetAsync(A, 0, sizeof(double) * c->nvec, c->stream));
+  double *rv = A;  // field 0 of A: the forward transform takes it from there
+  k_densities<<<nb, 256, 0, c->stream>>>(G, c->m, T, c->v64, pd.beta, pd.closure, c->d_charge, pd.rho, h[0], h[1],
+                                         h[2], pd.L[0], pd.L[1], pd.L[2], c->n, c->d_solute, rv, ru);
+  CKL();
+  k_coulomb_long<<<nb, 256, 0, c->stream>>>(G, h[0], h[1], h[2], pd.L[0], pd.L[1], pd.L[2], c->n, c->d_solute, uc);
+  CKL();
+  double mu[13], mv[13];
+  moments_of(c, ru, 1, 0.0, 1.0, mu);
+  moments_of(c, rv, 1, 0.0, 1.0, mv);
+  const int rb = (int)std::min<long long>(2 * 148, (G.Nr + 255) / 256);
+  double *dpart = dalloc<double>(rb);
+  k_dot<<<rb, 256, 0, c->stream>>>(G.Nr, uc, rv, dpart);
+  CKL();
+  std::vector<double> hd(rb);
+  CK(cudaMemcpyAsync(hd.data(), dpart, sizeof(double) * rb, cudaMemcpyDeviceToHost, c->stream));
+  // spectra: Rv kept aside, Ru left in W
+  fwd3d(c, A);
+  CK(cudaMemcpyAsync(Rv, c->work<double>(), sizeof(double2) * G.Nc, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(A, ru, sizeof(double) * G.Nr, cudaMemcpyDeviceToDevice, c->stream));
+  fwd3d(c, A);
+  // points: the solute sites, then the 8 grid nodes around each
+  const int n = c->n;
+  std::vector<double3> pts;
+  std::vector<double> fr(3 * (size_t)n);
+  for (int u = 0; u < n; ++u) {
+    double y[3];
+    for (int d = 0; d < 3; ++d) y[d] = (c->solute[u].x[d] + pd.L[d] / 2) / h[d];
+    pts.push_back(make_double3(y[0], y[1], y[2]));
+  }
+  for (int u = 0; u < n; ++u) {
+    const double3 y = pts[u];
+    const double fl[3] = {std::floor(y.x), std::floor(y.y), std::floor(y.z)};
+    fr[3 * u] = y.x - fl[0];
+    fr[3 * u + 1] = y.y - fl[1];
+    fr[3 * u + 2] = y.z - fl[2];
+    for (int q = 0; q < 8; ++q) pts.push_back(make_double3(fl[0] + (q & 1), fl[1] + ((q >> 1) & 1), fl[2] + (q >> 2)));
+  }
+  const int npts = (int)pts.size();
+  double3 *dpts = dalloc<double3>(std::max(npts, 1));
+  if (npts) CK(cudaMemcpyAsync(dpts, pts.data(), sizeof(double3) * npts, cudaMemcpyHostToDevice, c->stream));
+  const long long nk = (long long)G.Nh * G.N1 * G.N2;
+  const int kb = (int)std::min<long long>(2 * 148, (nk + 255) / 256);
+  double *kpart = dalloc<double>((size_t)kb * (npts + 1));
+  k_info_kspace<<<dim3(kb, npts + 1), 256, 0, c->stream>>>(G, Rv, c->work<double>(), npts, dpts, kpart);
+  CKL();
+  std::vector<double> hk((size_t)kb * (npts + 1));
+  CK(cudaMemcpyAsync(hk.data(), kpart, sizeof(double) * hk.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaEventRecord(e1, c->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (void *p : {(void *)A, (void *)ru, (void *)uc, (void *)Rv, (void *)dpart, (void *)dpts, (void *)kpart}) dfree(p);
+  const double Ntot = (double)G.Nr;
+  std::vector<double> val(npts + 1, 0.0);
+  for (int q = 0; q <= npts; ++q)
+    for (int b = 0; b < kb; ++b) val[q] += hk[(size_t)q * kb + b];
+  for (int q = 0; q < npts; ++q) val[q] /= Ntot;
+  res->q_u = mu[0];
+  res->q_v = mv[0];
+  for (int d = 0; d < 3; ++d) {
+    res->d_u[d] = mu[1 + d];
+    res->d_v[d] = mv[1 + d];
+    for (int e = 0; e < 3; ++e) {
+      res->Q_u[d][e] = mu[4 + 3 * d + e];
+      res->Q_v[d][e] = mv[4 + 3 * d + e];
+    }
+  }
+  for (int u = 0; u < n; ++u)
+    for (int d = 0; d < 3; ++d) res->d_n[d] += c->solute[u].charge * c->solute[u].x[d];
+  double v1 = 0.0, v1l = 0.0;
+  for (int u = 0; u < n; ++u) {
+    const double q = c->solute[u].charge;
+    v1 += q * val[u];
+    double t = 0.0;
+    for (int k = 0; k < 8; ++k) {
+      const double wx = (k & 1) ? fr[3 * u] : 1 - fr[3 * u];
+      const double wy = ((k >> 1) & 1) ? fr[3 * u + 1] : 1 - fr[3 * u + 1];
+      const double wz = (k >> 2) ? fr[3 * u + 2] : 1 - fr[3 * u + 2];
+      t += wx * wy * wz * val[n + 8 * u + k];
+    }
+    v1l += q * t;
+    if (site_potential) site_potential[u] = val[u];
+  }
+  res->U_v_rho_N = v1;
+  res->U_v_rho_N_trilinear = v1l;
+  // Parseval: h^3 sum v_e rho_u = (h^3 / N) sum_k V conj(Ru) over the full spectrum
+  res->U_v_rho_u = c->h3 * val[npts] / Ntot;
+  double d3 = 0.0;
+  for (double x : hd) d3 += x;
+  res->rho_v_U_u = c->h3 * d3;
+  res->seconds = ms * 1e-3;
+  return RISM3D_OK;
+}
+
 // One solve on a fresh context from host buffers (rism3d_solute_solve).
 int solve_on(rism3d_ctx *ctx, double *t_inout, double *g_out, rism3d_result *out) {
   const size_t bytes = sizeof(double) * ctx->nvec;
@@ -2379,6 +2518,20 @@ int rism3d_solute_solve(const rism3d_problem *pd, int m, const rism3d_site *solv
   rism3d_ctx_destroy(ctx);
   if (out && rc < 0 && out->status == 0) out->status = rc;
   return rc;
+}
+
+int rism3d_info(rism3d_ctx *ctx, const double *T, rism3d_info_result *out, double *site_potential) {
+  if (!ctx || !T || !out) return RISM3D_ERR_ARG;
+  if (ctx->pure) return RISM3D_ERR_UNSUPPORTED;
+  return guard([&] { return info_impl(ctx, T, out, site_potential); });
+}
+
+int rism3d_moments(rism3d_ctx *ctx, const double *g, int fields, double *out) {
+  if (!ctx || !g || !out || fields < 1) return RISM3D_ERR_ARG;
+  return guard([&] {
+    moments_of(ctx, g, fields, 1.0, -1.0, out);
+    return RISM3D_OK;
+  });
 }
 
 int rism3d_ctx_create_chi3(const rism3d_problem *pd, int m, const rism3d_site *solvent, int n,

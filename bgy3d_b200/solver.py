@@ -426,6 +426,38 @@ class RismContext:
                    "response")
         return {"x": arrs["x"], "krylov-jv": g.adjoint_jv, "resid": g.adjoint_resid, "seconds": g.seconds}
 
+    def info(self, T):
+        """Post-processing observables at a converged T (rism3d_info, the
+        reference's print_info): charge, dipole and second moments of the
+        solute ("q_u", "d_u", "Q_u") and solvent ("q_v", ...) charge
+        densities, the cores' dipole "d_n", and the energies "U_v_rho_N"
+        (trigonometric interpolation), "U_v_rho_N_trilinear", "U_v_rho_u",
+        "rho_v_U_u"; "site_potential" [n]."""
+        r = _abi.InfoResult()
+        vs = np.zeros(max(self.n, 1))
+        _abi.check(_abi.lib().rism3d_info(self._h, self._check_vec(T, self._torch.float64), ctypes.byref(r),
+                                          _dptr(vs)), "rism3d_info")
+        out = {k: getattr(r, k) for k in ("q_u", "q_v", "U_v_rho_N", "U_v_rho_N_trilinear", "U_v_rho_u",
+                                          "rho_v_U_u", "seconds")}
+        for k in ("d_u", "d_v", "d_n"):
+            out[k] = np.array(getattr(r, k)[:])
+        for k in ("Q_u", "Q_v"):
+            out[k] = np.array([list(row) for row in getattr(r, k)])
+        out["site_potential"] = vs[:self.n]
+        return out
+
+    def moments(self, g):
+        """Moments of 1 - g for each field of g (a CUDA FP64 tensor of whole
+        fields on this grid): list of (q, d[3], Q[3][3]) (rism3d_moments)."""
+        t = self._torch
+        n1 = self.shape[1] * self.shape[2] * self.shape[3]
+        if not (g.is_cuda and g.dtype == t.float64 and g.is_contiguous() and g.numel() % n1 == 0):
+            raise ValueError("expected a contiguous CUDA float64 tensor of whole fields")
+        nf = g.numel() // n1
+        out = np.zeros((nf, 13))
+        _abi.check(_abi.lib().rism3d_moments(self._h, ctypes.c_void_p(g.data_ptr()), nf, _dptr(out)), "rism3d_moments")
+        return [(o[0], o[1:4].copy(), o[4:].reshape(3, 3).copy()) for o in out]
+
     def observables(self, T, want_g=False):
         res = _abi.Result()
         g = self.zeros() if want_g else None

@@ -319,6 +319,39 @@ int rism3d_profile(rism3d_ctx *ctx, int on, double *ms, long long *launches);
 int rism3d_jacobian_apply_noalloc(const rism3d_problem *pd, int m, const double *chi,
                                   const double *d, const double *dT, double *JdT);
 
+/* ---- post-processing observables --------------------------------------- */
+
+/* What print_info writes after a solute solve (info(), bgy3d-potential.c:
+   245-493): moments of the solute's Gaussian charge density rho_u (cores(),
+   bgy3d-solutes.c:555-577) and of the solvent charge density rho_v = rho
+   sum_i q_i g_i (bgy3d_solvent_field), and three electrostatic energies with
+   the solvent's Poisson potential v_e (bgy3d_poisson, bgy3d-poisson.c:
+   103-183; no metallic cage).  Moments as bgy3d_moments (bgy3d-vec.c:
+   576-593): q = h^3 sum f, d_a = h^3 h_a sum f x_a, Q_ab = h^3 h_a h_b sum
+   f x_a x_b with x_a the grid index minus N_a / 2. */
+typedef struct rism3d_info_result {
+  double q_u, d_u[3], Q_u[3][3];  /* solute charge density */
+  double q_v, d_v[3], Q_v[3][3];  /* solvent charge density */
+  double d_n[3];                  /* dipole sum q x of the solute's point charges */
+  double U_v_rho_N;               /* sum_u q_u v_e(x_u), trigonometric interpolation (bgy3d_pot_interp) */
+  double U_v_rho_N_trilinear;     /* the same with trilinear interpolation (bgy3d_interp,
+                                     bgy3d-interp.c:37-136; the value the regression outputs hold) */
+  double U_v_rho_u;               /* h^3 sum v_e rho_u */
+  double rho_v_U_u;               /* h^3 sum u_c rho_v, u_c the solute's long-range Coulomb */
+  double seconds;
+} rism3d_info_result;
+
+/* The observables at a converged T (FP64 device pointer) of a solute
+   context; site_potential (host [n] or NULL) receives v_e at the solute
+   sites (trigonometric, print_table's column). */
+int rism3d_info(rism3d_ctx *ctx, const double *T, rism3d_info_result *out, double *site_potential);
+
+/* Moments of 1 - g for `fields` distributions g (device, [fields][N2][N1]
+   [N0] on the context's grid): the `moments` command of the regression
+   summaries (guile/bgy3d.scm:1136-1155).  out: host [fields][13] = q, d[3],
+   Q[3][3] per field. */
+int rism3d_moments(rism3d_ctx *ctx, const double *g, int fields, double *out);
+
 /* ---- 3D solvent susceptibility (the --solvent-3d path) ---------------- */
 
 /* Results of the pure-solvent solve. */

@@ -80,6 +80,33 @@ def test_pure_water_matches_goldens(solvent_run):
     assert np.all(np.isfinite(r["GVV"])) and r["compressibility"] > 0
 
 
+def regression():
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "hnc3d_regression.json")) as f:
+        return json.load(f)
+
+
+def check_moments(got, gold):
+    """4 printed digits: within half a unit of the last one."""
+    q, d, Q = got
+    assert abs(q - gold["q"]) <= 5e-5 + 1e-9
+    assert np.max(np.abs(d - np.array(gold["d"]))) <= 5e-5 + 1e-9
+    assert np.max(np.abs(Q - np.array(gold["Q"]))) <= 5e-5 + 1e-9
+
+
+def test_pure_water_g_moments(solvent_run):
+    w, r = solvent_run
+    ctx = RismContext(None, w, SETTINGS, None)
+    mom = ctx.moments(torch.tensor(r["GVV"], device="cuda"))
+    ctx.close()
+    pair = {"g00.bin": 0, "g01.bin": 1, "g11.bin": 2, "g02.bin": 3, "g12.bin": 4, "g22.bin": 5}
+    gold = regression()["solvent"]["moments"]
+    assert len(gold) == 6
+    for gm in gold:
+        check_moments(mom[pair[gm["file"]]], gm)
+
+
 @pytest.mark.parametrize("name", list(GOLDEN_SOLUTE))
 def test_solutes_in_3d_solvent_match_goldens(solvent_run, name):
     w, r = solvent_run
@@ -92,3 +119,37 @@ def test_solutes_in_3d_solvent_match_goldens(solvent_run, name):
     if name == "water":
         for got, orc in zip(mu, ORACLE_WATER):
             assert abs(got - orc) < 1e-8
+
+
+@pytest.mark.parametrize("name", list(GOLDEN_SOLUTE))
+def test_solute_observables_match_goldens(solvent_run, name):
+    """print_info's observables and the moments of 1 - g of the same runs."""
+    w, r = solvent_run
+    gold = regression()["solutes"][name]
+    ctx = RismContext(find_molecule(name), w, SETTINGS, r["susceptibility-3d"])
+    T, res = ctx.solve()
+    assert res["status"] == 0
+    inf = ctx.info(T)
+    g = ctx.observables(T, want_g=True)["GUV"]
+    mom = ctx.moments(g)
+    ctx.close()
+    gi = gold["info"]
+    tol = 5e-7 + 1e-9  # 6 printed digits
+    assert abs(inf["q_u"]) <= tol and abs(inf["q_v"]) <= tol
+    for key in ("d_n", "d_u", "d_v"):
+        assert np.max(np.abs(inf[key] - np.array(gi[key]))) <= tol, (name, key, inf[key])
+    assert abs(inf["U_v_rho_N_trilinear"] - gi["U_v_rho_N"]) <= tol, (name, inf["U_v_rho_N_trilinear"])
+    assert abs(inf["U_v_rho_u"] - gi["U_v_rho_u"]) <= tol, (name, inf["U_v_rho_u"])
+    assert abs(inf["rho_v_U_u"] - gi["rho_v_U_u"]) <= tol, (name, inf["rho_v_U_u"])
+    files = {m["file"]: m for m in gold["moments"]}
+    for i in range(3):
+        check_moments(mom[i], files["g%d.bin" % i])
+    if name == "water":
+        # the trigonometric value (the shipped bgy3d_pot_interp) and the rest
+        # against the oracle on the same g
+        from oracle import info as oinfo
+        ref = oinfo.info((96,) * 3, (20.0,) * 3, SETTINGS["rho"], w, find_molecule(name), g.cpu().numpy())
+        for key in ("U_v_rho_N", "U_v_rho_N_trilinear", "U_v_rho_u", "rho_v_U_u", "q_v"):
+            assert abs(inf[key] - ref[key]) < 1e-9 * max(1.0, abs(ref[key])), key
+        assert np.max(np.abs(inf["Q_v"] - ref["Q_v"])) < 1e-9
+        assert np.max(np.abs(inf["site_potential"] - ref["site_potential"])) < 1e-9

@@ -155,3 +155,25 @@ def test_3d_solvent_water_solute_golden(solvent3d_water):
     assert abs(mu["HNC"] - -2.284209) < 5e-7
     assert abs(mu["KH"] - -3.894980) < 5e-7
     assert abs(mu["GF"] - -5.870259) < 5e-7
+    # print_info's observables and the moments of 1 - g (test/out/water.hnc3d.g1)
+    from oracle import info
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "hnc3d_regression.json")) as f:
+        gold = json.load(f)
+    gi = gold["solutes"]["water"]["info"]
+    got = info.info((96,) * 3, (20.0,) * 3, 0.033427745, w, w, res["g"])
+    assert abs(got["U_v_rho_N_trilinear"] - gi["U_v_rho_N"]) < 5e-7
+    assert abs(got["U_v_rho_u"] - gi["U_v_rho_u"]) < 5e-7
+    assert abs(got["rho_v_U_u"] - gi["rho_v_U_u"]) < 5e-7
+    assert np.max(np.abs(got["d_v"] - np.array(gi["d_v"]))) < 5e-7
+    for i, gm in enumerate(gold["solutes"]["water"]["moments"]):
+        q, d, Q = info.g_moments(res["g"][i], (96,) * 3, (20.0,) * 3)
+        assert abs(q - gm["q"]) < 5e-5
+        assert np.max(np.abs(d - np.array(gm["d"]))) < 5e-5
+        assert np.max(np.abs(Q - np.array(gm["Q"]))) < 5e-5
+    pair = {"g00.bin": 0, "g01.bin": 1, "g11.bin": 2, "g02.bin": 3, "g12.bin": 4, "g22.bin": 5}
+    for gm in gold["solvent"]["moments"]:
+        q, d, Q = info.g_moments(out["g"][pair[gm["file"]]], (96,) * 3, (20.0,) * 3)
+        assert abs(q - gm["q"]) < 5e-5
+        assert np.max(np.abs(Q - np.array(gm["Q"]))) < 5e-5
