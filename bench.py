@@ -26,7 +26,12 @@ sites on grids 64^3..192^3 solved by rism3d_solve_batch in mixed and FP64
 precision (aggregate solves/s, per-solute |dmu|); "gradient", the adjoint
 dmu/d(q, sigma, eps, x) of the workload's solute (time against one
 solve, central-difference checks); "pes", an 8-point scan of the solute
-rebound on one context with warm starts, against fresh solves.
+rebound on one context with warm starts, against fresh solves;
+"cufft_yardstick", the Jacobian product against a cuFFT (torch.fft) form of
+it, speed and max difference.
+
+  python bench.py --large           the 512^3 / 150-site single solve
+                                    (mixed against plain FP64)
 
   python bench.py --profile-solve   one warm mixed solve between
                                     cudaProfilerStart/Stop (for ncu
@@ -100,9 +105,15 @@ def run_batch_report(solvent, s, chi, count=64, workers=8):
     solutes, sets = batch_workload(count, s)
     out = {}
     mus = {}
+    # warm: one solute of every grid (the pass-schedule autotuner times each
+    # new grid shape once per process, like an FFT plan)
+    first = {}
+    for i, x in enumerate(sets):
+        first.setdefault(x["N"], i)
+    warm = sorted(first.values())
     for prec in ("mixed", "fp64"):
         st = [dict(x, precision=prec) for x in sets]
-        hnc3d_run_batch(solutes[:workers], solvent, st[:workers], chi, workers=workers)  # warm
+        hnc3d_run_batch([solutes[i] for i in warm], solvent, [st[i] for i in warm], chi, workers=workers)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         res = hnc3d_run_batch(solutes, solvent, st, chi, workers=workers)
@@ -191,6 +202,131 @@ def run_pes_report(solute, solvent, s, chi, points=8, step=0.05):
     return {"points": points, "step_A": step, "rebind_warm_solves_per_s": points / warm,
             "fresh_solves_per_s": points / fresh, "newton_per_point": iters,
             "timing": "host clock around the scan"}
+
+
+def run_cufft_yardstick(solute, solvent, s, chi, reps=5):
+    """cuFFT as a speed and accuracy yardstick for the Jacobian product (the
+    evaluation a plain FP64 solve makes 464 of): J dT = (chi-1) * (c'(T) dT)
+    - dT written with torch.fft (cuFFT) and dense k-grid chi tables, against
+    rism3d_jacobian_t1 on the same T (the workload's field at t = 0) and a
+    seeded dT.  Device time per product (CUDA events) and the max |difference|."""
+    import torch
+    from bgy3d_b200 import RismContext
+    ctx = RismContext(solute, solvent, s, chi)
+    N, Lf = s["N"], 2 * s["L"]
+    m = len(solvent)
+    T = ctx.zeros()
+    v = ctx.field(0)
+    beta = s["beta"]
+    x = -beta * v + T
+    d = torch.where(x <= 0, torch.expm1(torch.clamp(x, max=0.0)), torch.zeros_like(x))  # KH slope
+    g = torch.Generator(device="cuda").manual_seed(7)
+    dT = torch.randn(T.shape, generator=g, device="cuda", dtype=torch.float64) * 1e-2
+    # chi - 1 on the r2c grid by the reference's radial rule (bgy3d-vec.c:22-46)
+    dk = 2 * np.pi / Lf
+    kx = torch.arange(N // 2 + 1, device="cuda", dtype=torch.float64)
+    ky = torch.fft.fftfreq(N, 1.0 / N, device="cuda", dtype=torch.float64)
+    kk = torch.sqrt((kx[None, None, :] * dk) ** 2 + (ky[None, :, None] * dk) ** 2 + (ky[:, None, None] * dk) ** 2)
+    nrad, dkr = chi.shape[-1], np.pi / s["rmax"]
+    ix = kk / dkr - 0.5
+    i = torch.clamp(torch.floor(ix + 0.5).long(), 0, nrad - 1)
+    ip = torch.where(i < nrad - 2, i + 1, i)
+    im = torch.where(i > 1, i - 1, i)
+    tabs = torch.tensor(chi, device="cuda", dtype=torch.float64) - torch.eye(m, device="cuda", dtype=torch.float64)[
+        :, :, None]
+    K = torch.empty((m, m) + kk.shape, device="cuda", dtype=torch.float64)
+    for a in range(m):
+        for b in range(m):
+            t = tabs[a, b]
+            K[a, b] = t[i] + (t[ip] - t[im]) / (ip - im).to(torch.float64) * (ix - i)
+
+    def jv_cufft(dt, dd, KK):
+        c = torch.fft.rfftn(dd * dt, dim=(-3, -2, -1))
+        re = torch.einsum("abxyz,bxyz->axyz", KK, c.real)
+        im = torch.einsum("abxyz,bxyz->axyz", KK, c.imag)
+        return torch.fft.irfftn(torch.complex(re, im), s=(N, N, N), dim=(-3, -2, -1)) - dt
+
+    out = {}
+    for name, dt_ in (("f64", torch.float64), ("f32", torch.float32)):
+        Tq, dTq, dq, Kq = T.to(dt_), dT.to(dt_), d.to(dt_), K.to(dt_)
+        ours = ctx.jacobian_t1(Tq, dTq)
+        ref = jv_cufft(dTq, dq, Kq)
+        torch.cuda.synchronize()
+        times = {}
+        for label, fn in (("ours", lambda: ctx.jacobian_t1(Tq, dTq, out=ours)), ("cufft", lambda: jv_cufft(dTq, dq, Kq))):
+            fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(reps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            times[label] = e0.elapsed_time(e1) / reps
+        diff = float((ours.double() - ref.double()).abs().max())
+        scale = float(ref.double().abs().max())
+        out[name] = {"ms_ours": times["ours"], "ms_cufft": times["cufft"], "ours_over_cufft_speed":
+                     times["cufft"] / times["ours"], "max_abs_diff": diff, "max_rel_diff": diff / scale}
+        del Tq, dTq, dq, Kq, ours, ref
+    ctx.close()
+    out["note"] = ("J.v at 256^3 on the workload's T = 0: ours = rism3d_jacobian_t1 (5 fused passes); cufft = "
+                   "torch.fft rfftn/irfftn + einsum with dense k-grid chi tables (yardstick only, not a product path)")
+    return out
+
+
+def run_large(args):
+    """The large single solve: a 150-site synthetic neutral solute (seed
+    20261203, sites in a 14 A ball) in PR-SPC/E water on a 512^3 grid with
+    half edge 48 A (96 A box, h = 0.1875 A), mixed precision to |F|inf <
+    1e-10 against the plain FP64 form; device time, peak device memory of
+    the library's pool and per-pass HBM rates of one mixed solve."""
+    import torch
+    from bgy3d_b200 import RismContext, find_molecule, rism_solvent, synthetic_solute
+    solvent = find_molecule("water, PR-SPC/E")
+    solute = synthetic_solute(150, radius=14.0, seed=20261203)
+    s = dict(SETTINGS, N=512, L=48.0)
+    chi = rism_solvent(solvent, dict(s, **{"norm-tol": 1e-12}))["susceptibility"]
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    out = {"workload": "150-site synthetic neutral solute (14 A ball) in PR-SPC/E water, 512^3 grid, 96 A box, KH, "
+                       "|F|inf < 1e-10", "grid": 512, "solute_sites": 150}
+    for label, st in (("mixed", {"precision": "mixed"}), ("fp64_plain", PLAIN_FP64)):
+        ctx = RismContext(solute, solvent, dict(s, **st), chi)
+        T = ctx.zeros()
+        if label == "mixed":  # one untimed solve (graph capture, Krylov buffers)
+            ctx.solve(T)
+            T.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        _, res = ctx.solve(T)
+        e1.record()
+        torch.cuda.synchronize()
+        obs = ctx.observables(T)
+        free1, _ = torch.cuda.mem_get_info()
+        out[label] = {"seconds": e0.elapsed_time(e1) * 1e-3, "mu": obs["free-energy"], "status": res["status"],
+                      "resid_inf": res["resid-inf"], "newton": res["newton-iters"],
+                      "jv_evals": res["jv-evals"] + res["jv-evals-fp32"], "jv_evals_coarse": res["jv-evals-coarse"],
+                      "device_memory_gb": (free0 - free1) / 1e9}
+        if label == "mixed":
+            ctx.profile(True)  # a third solve with per-pass event timing
+            T.zero_()
+            ctx.solve(T)
+            prof = ctx.profile(False)
+            lau = {k: prof[(k, "f32")][1] for k in ("xfwd", "y", "z", "xinv")}
+            byt = pass_bytes(512, 3, 4, lau, res["f-evals-fp32"])
+            out[label]["pass_gbs_f32"] = {k: byt[k] / (prof[(k, "f32")][0] * 1e-3) / 1e9
+                                          for k in lau if prof[(k, "f32")][0] > 0}
+            out[label]["passes_ms"] = {f"{a}/{p}": round(v[0], 1) for (a, p), v in prof.items() if v[1]}
+            out[label]["tile_shapes"] = ctx.tile_shapes()
+        ctx.close()
+        del T
+        torch.cuda.synchronize()
+    out["speedup_vs_plain_fp64"] = out["fp64_plain"]["seconds"] / out["mixed"]["seconds"]
+    out["dmu_vs_fp64_plain"] = out["mixed"]["mu"] - out["fp64_plain"]["mu"]
+    out["device_memory_note"] = "free device memory before the first context minus after each solve (the pool " \
+                                "keeps its high-water mark)"
+    print(json.dumps(out))
 
 
 def config(grid=GRID, precision="mixed"):
@@ -391,9 +527,15 @@ def run_ours(args, rank, world):
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, sample_evals=1)
     if world == 1 and not args.no_extras:
-        line["batch"] = run_batch_report(solvent, s, chi)
-        line["gradient"] = run_gradient_report(solute, solvent, s, chi, ms / args.steps)
-        line["pes"] = run_pes_report(solute, solvent, s, chi)
+        extras = (("batch", lambda: run_batch_report(solvent, s, chi)),
+                  ("gradient", lambda: run_gradient_report(solute, solvent, s, chi, ms / args.steps)),
+                  ("pes", lambda: run_pes_report(solute, solvent, s, chi)),
+                  ("cufft_yardstick", lambda: run_cufft_yardstick(solute, solvent, dict(s, precision="mixed"), chi)))
+        for key, fn in extras:
+            try:
+                line[key] = fn()
+            except Exception as e:  # an extra report never costs the timed line
+                line[key] = {"error": f"{type(e).__name__}: {e}"}
     return line
 
 
@@ -517,6 +659,8 @@ def main():
                     help="skip the many-solute batch and gradient reports")
     ap.add_argument("--evals", type=int, default=0,
                     help="profiling mode: time this many F and J.v evaluations instead of solves")
+    ap.add_argument("--large", action="store_true",
+                    help="the 512^3 / 150-site single solve against plain FP64 (prints its own line)")
     ap.add_argument("--profile-solve", action="store_true",
                     help="profiling mode: one warm mixed solve between cudaProfilerStart/Stop")
     args = ap.parse_args()
@@ -525,6 +669,9 @@ def main():
         return
     if args.profile_solve:
         run_profile_solve(args)
+        return
+    if args.large:
+        run_large(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

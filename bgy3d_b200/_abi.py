@@ -13,8 +13,8 @@ LIB_PATH = os.path.join(HERE, "librism3d.so")
 HNC, KH, PY = 0, 1, 2
 PSE0 = 3
 CLOSURES = {"HNC": 0, "KH": 1, "PY": 2, **{f"PSE{n}": 3 + n for n in range(8)}}
-NEWTON, PICARD, TRIAL = 0, 1, 2
-SOLVERS = {"newton": NEWTON, "picard": PICARD, "trial": TRIAL}
+NEWTON, PICARD, TRIAL, JAGER = 0, 1, 2, 3
+SOLVERS = {"newton": NEWTON, "picard": PICARD, "trial": TRIAL, "jager": JAGER}
 FP64, MIXED = 0, 1
 
 OK = 0
@@ -95,7 +95,7 @@ EXPORTS = [
     "rism3d_precondition", "rism3d_coarse_grid", "rism3d_solve_batch",
     "rism3d_solute_grad", "rism3d_gradient", "rism3d_jacobian_transpose_t1", "rism3d_ctx_set_solute",
     "rism3d_response", "rism3d_solvent_solve", "rism3d_solvent_ctx_create", "rism3d_ctx_create_chi3",
-    "rism3d_solute_solve_chi3", "rism3d_info", "rism3d_moments",
+    "rism3d_solute_solve_chi3", "rism3d_info", "rism3d_moments", "rism3d_tile_shapes",
 ]
 
 _lib = None
@@ -168,6 +168,8 @@ def lib():
     L.rism3d_info.restype = I
     L.rism3d_moments.argtypes = [V, V, I, P(D)]
     L.rism3d_moments.restype = I
+    L.rism3d_tile_shapes.argtypes = [V, P(I)]
+    L.rism3d_tile_shapes.restype = I
     _lib = L
     return L
 

@@ -17,10 +17,12 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <numeric>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "kernels.cuh"
@@ -1224,7 +1226,8 @@ int solve_impl(rism3d_ctx *c, double *T, rism3d_result *out) {
   NewtonOut o;
   int status = RISM3D_OK;
   const rism3d_problem &pd = c->pd;
-  if (pd.closure == RISM3D_PY && pd.solver != RISM3D_PICARD) {
+  const bool mixing = pd.solver == RISM3D_PICARD || pd.solver == RISM3D_JAGER;  // no Jacobian
+  if (pd.closure == RISM3D_PY && !mixing) {
     CK(cudaEventDestroy(e0));
     CK(cudaEventDestroy(e1));
     return RISM3D_ERR_UNSUPPORTED;
@@ -1244,7 +1247,42 @@ int solve_impl(rism3d_ctx *c, double *T, rism3d_result *out) {
     o.rinf = r[0];
     o.r2 = r[1];
   }
-  if (pd.solver != RISM3D_PICARD) {
+  if (pd.solver == RISM3D_JAGER) {
+    // bgy3d_snes_jager (bgy3d-snes.c:402-509): x += a F(x), where a is the
+    // "move" coefficient a1 every 10th iteration and lambda otherwise; a1
+    // doubles (up to 1) after 20 quiet iterations and halves (down to
+    // lambda) when a move made an otherwise falling norm go up.
+    const double a0 = pd.lambda;
+    double a1 = pd.lambda, norm_old = 0.0;
+    int mycount = 0, upwards = 0;
+    const int nth = 10;
+    double *F = xbuf<double>(c, 0);
+    double r[2] = {0, 0};
+    for (int iter = 0; iter < pd.max_iter; ++iter) {
+      eval_F<double>(c, T, F, r);
+      const double norm = r[0];
+      const double a = (iter % nth == 0) ? a1 : a0;
+      xpay<double, double, double>(c, T, a, F, T);
+      const bool up = norm > norm_old;
+      norm_old = norm;
+      mycount++;
+      if (iter % nth != 1) upwards = up ? 1 : 0;
+      if (iter % nth == 1 && up && upwards == 0 && iter > 2 * nth) {
+        a1 = std::max(a1 / 2.0, a0);
+        mycount = 0;
+      }
+      if (mycount > 2 * nth) {
+        a1 = std::min(a1 * 2.0, 1.0);
+        mycount = 0;
+      }
+      o.iters = iter + 1;
+      if (!(norm == norm)) { o.nan = true; break; }
+      if (norm <= pd.norm_tol) { o.converged = true; break; }
+    }
+    o.rinf = r[0];
+    o.r2 = r[1];
+  }
+  if (!mixing) {
     if (pd.precision == RISM3D_MIXED) {
       // FP32 bulk: Newton on a float copy of t until the float residual floor.
       if (!c->X32) c->X32 = dalloc<float>(c->nvec);
@@ -1589,6 +1627,131 @@ void bind_solute(rism3d_ctx *c, int n, const rism3d_site *solute) {
   if (c->coarse) bind_solute(c->coarse, n, solute);
 }
 
+// ------------------------------------------------------------ autotuner
+// The batch sizes of the runtime-length passes (x rows, y and z columns per
+// CTA) and, where shape-specialised passes exist, the choice between them and
+// the runtime-length ones are timed on the context's own buffers the first
+// time a (grid, fields) shape is seen in the process; the winners are cached.
+// Only the scheduling changes: every candidate computes the same transforms
+// column by column.  RISM3D_AUTOTUNE=0 keeps the register / occupancy rule.
+struct TuneVal {
+  TileShape t[2];
+  bool stat[2];
+};
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int>, TuneVal> g_tune;
+
+int optin_limit() {
+  int dev = 0, optin = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  return optin - 4096;  // margin for the kernels' static shared memory
+}
+
+template <typename F> float time_ms(rism3d_ctx *c, F &&f, int reps) {
+  f();  // warm
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  CK(cudaEventRecord(a, c->stream));
+  for (int i = 0; i < reps; ++i) f();
+  CK(cudaEventRecord(b, c->stream));
+  CK(cudaEventSynchronize(b));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return ms / reps;
+}
+
+template <typename T> void tune_precision(rism3d_ctx *c, const T *A, const T *Bv, T *out) {
+  const int pr = sizeof(T) == 8 ? 0 : 1;
+  const Geo &G = c->g;
+  TileShape &t = c->tiles[pr];
+  const int rc = pr == 0 ? reg_complex<double2>() : reg_complex<float2>();
+  const size_t cs = sizeof(typename Cx<T>::type);
+  const long long lim = optin_limit();
+  const int reps = G.Nr >= (1LL << 22) ? 2 : 5;
+  const bool had_stat = c->stat[pr];
+  c->stat[pr] = false;
+  auto run = [&] { pipeline<T, MODE_J>(c, A, Bv, (T)1, (T)1, out); };
+  const int cand[4] = {4, 8, 16, 32};
+  // one axis at a time, the others held
+  int *fields[3] = {&t.RX, &t.BY, &t.BZ};
+  for (int axis = 0; axis < 3; ++axis) {
+    int best = *fields[axis];
+    float best_ms = time_ms(c, run, reps);
+    for (int k : cand) {
+      if (k == best) continue;
+      long long smem;
+      if (axis == 0) {
+        if (G.M * k > rc * 256 || (k > 16)) continue;
+        smem = (long long)cs * (G.M + k * G.M);
+      } else if (axis == 1) {
+        if (G.N1 * k > rc * 256 || k > 16) continue;
+        smem = (long long)cs * (G.N1 + G.N1 * k);
+      } else {
+        if (G.N2 * k > rc * 256 || k > 16) continue;
+        smem = (long long)cs * (G.N2 + (long long)G.N2 * G.m * k);
+      }
+      if (smem > lim) continue;
+      const int keep = *fields[axis];
+      *fields[axis] = k;
+      const float ms = time_ms(c, run, reps);
+      if (ms < best_ms) { best_ms = ms; best = k; }
+      *fields[axis] = keep;
+    }
+    *fields[axis] = best;
+  }
+  if (had_stat) {
+    const float g_ms = time_ms(c, run, reps);
+    c->stat[pr] = true;
+    const float s_ms = time_ms(c, run, reps);
+    c->stat[pr] = s_ms <= g_ms;
+  }
+}
+
+// Applies the cached shapes of this context's (grid, fields) or times them.
+void autotune(rism3d_ctx *c) {
+  const char *env = std::getenv("RISM3D_AUTOTUNE");
+  if (env && env[0] == '0') return;
+  const Geo &G = c->g;
+  const int kind = c->pure ? 2 : (c->chi3_64 ? 1 : 0);  // the z pass differs per kind
+  const auto key = std::make_tuple(G.N0, G.N1, G.N2, G.m, kind);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      for (int pr = 0; pr < 2; ++pr) {
+        c->tiles[pr] = it->second.t[pr];
+        c->stat[pr] = c->stat[pr] && it->second.stat[pr];
+      }
+      return;
+    }
+  }
+  const long long nv = c->nvec;
+  double *a64 = dalloc<double>(nv), *b64 = dalloc<double>(nv), *o64 = dalloc<double>(nv);
+  CK(cudaMemsetAsync(a64, 0, sizeof(double) * nv, c->stream));
+  CK(cudaMemsetAsync(b64, 0, sizeof(double) * nv, c->stream));
+  tune_precision<double>(c, a64, b64, o64);
+  if (!c->pure) {
+    float *a32 = reinterpret_cast<float *>(a64), *b32 = reinterpret_cast<float *>(b64);
+    tune_precision<float>(c, a32, b32, reinterpret_cast<float *>(o64));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  dfree(a64);
+  dfree(b64);
+  dfree(o64);
+  c->timer = PassTimer{};
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  TuneVal v;
+  for (int pr = 0; pr < 2; ++pr) {
+    v.t[pr] = c->tiles[pr];
+    v.stat[pr] = c->stat[pr];
+  }
+  g_tune[key] = v;
+}
+
 void check_grid(const rism3d_problem *pd) {
   for (int d = 0; d < 3; ++d) {
     if (!is_2a3b(pd->N[d]) || pd->N[d] % 2 || pd->N[d] < 8 || pd->N[d] > kMaxN)
@@ -1678,7 +1841,8 @@ void init_work(rism3d_ctx *c) {
   c->dpart = dalloc<double>((size_t)c->red_blocks * kVecMax + 64);
   c->dres = dalloc<double>(4 * kVecMax);
   const int rows = G.N1 * G.N2;
-  const int rxmin = std::min(std::min(c->tiles[0].RX, c->tiles[1].RX), kStaticRX);
+  // partials for the smallest x batch the tile autotuner may pick
+  const int rxmin = std::min(std::min(c->tiles[0].RX, c->tiles[1].RX), 4);
   c->npart = dalloc<NormPartial>((size_t)((rows + rxmin - 1) / rxmin) * G.m);
   c->d_err = dalloc<int>(1);
   CK(cudaMemset(c->d_err, 0, sizeof(int)));
@@ -1926,12 +2090,13 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
       OPTIN_S(float)
 #undef OPTIN_S
     }
+    autotune(c);
     // two-grid preconditioner: a copy of the problem on a coarse grid.  The
     // spacing coarse_h is taken when its grid has at most half the fine
     // points along every axis (a coarse solve costs ~12 coarse J.v per fine
     // iteration); otherwise 1 A (or coarse_h if coarser), when that grid is
     // still coarser than the fine one; otherwise the preconditioner is off.
-    if (pd->coarse_h > 0 && pd->solver != RISM3D_PICARD) {
+    if (pd->coarse_h > 0 && pd->solver != RISM3D_PICARD && pd->solver != RISM3D_JAGER) {
       auto grid_for = [&](double h, int *nc) {
         bool half = true;
         for (int a = 0; a < 3; ++a) {
@@ -2058,6 +2223,7 @@ int solvent_create_impl(const rism3d_problem *pd, int ms, const rism3d_site *sol
     CKL();
     dfree(dp);
     c->ck = dalloc<double2>((size_t)np * G.Nc);
+    CK(cudaMemsetAsync(c->ck, 0, sizeof(double2) * (size_t)np * G.Nc, c->stream));
     init_work(c);
     const size_t need = generic_smem(c);
     allow_xy(need);
@@ -2070,6 +2236,7 @@ int solvent_create_impl(const rism3d_problem *pd, int ms, const rism3d_site *sol
       case 3: allow_oz<3>(need); break;
       default: allow_oz<4>(need); break;
     }
+    autotune(c);
     CK(cudaStreamSynchronize(c->stream));
   } catch (...) {
     delete c;
@@ -2518,6 +2685,17 @@ int rism3d_solute_solve(const rism3d_problem *pd, int m, const rism3d_site *solv
   rism3d_ctx_destroy(ctx);
   if (out && rc < 0 && out->status == 0) out->status = rc;
   return rc;
+}
+
+int rism3d_tile_shapes(rism3d_ctx *ctx, int *out) {
+  if (!ctx || !out) return RISM3D_ERR_ARG;
+  for (int pr = 0; pr < 2; ++pr) {
+    out[3 * pr] = ctx->tiles[pr].RX;
+    out[3 * pr + 1] = ctx->tiles[pr].BY;
+    out[3 * pr + 2] = ctx->tiles[pr].BZ;
+    out[6 + pr] = ctx->stat[pr] ? 1 : 0;
+  }
+  return RISM3D_OK;
 }
 
 int rism3d_info(rism3d_ctx *ctx, const double *T, rism3d_info_result *out, double *site_potential) {

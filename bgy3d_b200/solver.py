@@ -376,6 +376,13 @@ class RismContext:
         _abi.check(_abi.lib().rism3d_ctx_set_solute(self._h, len(solute), _sites(solute)), "set_solute")
         self.n = len(solute)
 
+    def tile_shapes(self):
+        """The pass schedule chosen at creation (rism3d_tile_shapes):
+        {"f64": (RX, BY, BZ, shape-specialised), "f32": (...)}."""
+        out = (ctypes.c_int * 8)()
+        _abi.check(_abi.lib().rism3d_tile_shapes(self._h, out), "rism3d_tile_shapes")
+        return {"f64": (out[0], out[1], out[2], bool(out[6])), "f32": (out[3], out[4], out[5], bool(out[7]))}
+
     def coarse_grid(self):
         """Points per axis of the two-grid preconditioner's coarse grid
         (None when it is off)."""

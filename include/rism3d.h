@@ -34,7 +34,7 @@ enum {
 };
 
 /* Non-linear solvers, as --snes-solver (bgy3d-snes.c:16-35). */
-enum { RISM3D_NEWTON = 0, RISM3D_PICARD = 1, RISM3D_TRIAL = 2 };
+enum { RISM3D_NEWTON = 0, RISM3D_PICARD = 1, RISM3D_TRIAL = 2, RISM3D_JAGER = 3 };
 
 /* Arithmetic of the solve. */
 enum {
@@ -79,7 +79,7 @@ typedef struct rism3d_problem {
   int max_iter;       /* Newton iterations (PD->max_iter) */
   double norm_tol;    /* stop when ||F(t)||_inf < norm_tol */
   double lambda;      /* Picard mixing (PD->lambda) */
-  int solver;         /* RISM3D_NEWTON / _PICARD / _TRIAL */
+  int solver;         /* RISM3D_NEWTON / _PICARD / _TRIAL / _JAGER (bgy3d-snes.c:19-31) */
   int renorm;         /* 1: default; 0: --no-renorm (hnc3d.c:1607-1615) */
   int precision;      /* RISM3D_FP64 or RISM3D_MIXED */
   int verbosity;      /* 0 silent; 1 one line per Newton step on stderr */
@@ -288,6 +288,14 @@ int rism3d_gradient(rism3d_ctx *ctx, const double *T, rism3d_grad *grad);
    the largest ||beta K((c'+1)dv) - J dT||_2 / ||beta K((c'+1)dv)||_2, grad->
    seconds = device time.  PY has no closure differential: RISM3D_ERR_UNSUPPORTED. */
 int rism3d_response(rism3d_ctx *ctx, const double *T, rism3d_grad *grad);
+
+/* The pass schedule the context runs, written to out[8]: x rows, y and z
+   columns per CTA of the runtime-length passes for FP64 (out[0..2]) and
+   FP32 (out[3..5]), and whether the shape-specialised passes run (out[6]
+   FP64, out[7] FP32).  Chosen when the context is created by timing the
+   candidates on its own buffers, once per grid shape and process
+   (RISM3D_AUTOTUNE=0: a register / occupancy rule instead). */
+int rism3d_tile_shapes(rism3d_ctx *ctx, int *out);
 
 /* Points per axis of the two-grid preconditioner's coarse grid, written to
    n[3] (zeros when the preconditioner is off). */

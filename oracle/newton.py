@@ -67,3 +67,36 @@ def solve(F, x0, jv=None, tol=1e-12, max_iter=200, krylov_rtol=1e-3,
     if np.max(np.abs(f)) < tol:
         return x, max_iter
     raise NotConverged(f"no convergence: |F|inf = {np.max(np.abs(f)):.3e}")
+
+
+def jager(F, x0, lam, max_iter, tol):
+    """bgy3d_snes_jager (bgy3d-snes.c:402-509): x += a F(x) with the mixing
+    coefficient a = a1 every 10th iteration ("moves"), lambda otherwise; a1
+    doubles (up to 1) after 20 quiet iterations and halves back (not below
+    lambda) when a move made an otherwise falling norm go up.  Returns
+    (x, iterations, last |F|inf)."""
+    x = np.array(x0, dtype=np.float64, copy=True)
+    a0 = a1 = lam
+    norm_old = 0.0
+    mycount = upwards = 0
+    nth = 10
+    norm = np.inf
+    for it in range(max_iter):
+        dx = F(x)
+        norm = float(np.max(np.abs(dx)))
+        a = a1 if it % nth == 0 else a0
+        x += a * dx
+        up = norm > norm_old
+        norm_old = norm
+        mycount += 1
+        if it % nth != 1:
+            upwards = 1 if up else 0
+        if it % nth == 1 and up and upwards == 0 and it > 2 * nth:
+            a1 = max(a1 / 2.0, a0)
+            mycount = 0
+        if mycount > 2 * nth:
+            a1 = min(a1 * 2.0, 1.0)
+            mycount = 0
+        if norm <= tol:
+            return x, it + 1, norm
+    return x, max_iter, norm

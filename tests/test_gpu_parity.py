@@ -206,6 +206,24 @@ def test_picard_and_trial_solvers(fixture_loader):
         assert abs(out["free-energy"] - meta["mu"]) < 1e-6
 
 
+def test_jager_mixing_follows_the_reference_rule(fixture_loader):
+    """60 iterations of the adaptive mixing (bgy3d_snes_jager) from t = 0
+    land on the oracle's iterate of the same rule."""
+    from oracle import hnc3d, newton
+    meta, arr = fixture_loader("water_hnc_n24")
+    s = settings_of(meta, **{"snes-solver": "jager", "lambda": 0.1, "max-iter": 60, "norm-tol": 1e-14})
+    ctx = RismContext(meta["solute"], meta["solvent"], s, arr["chi"])
+    T, res = ctx.solve(ctx.zeros())
+    ctx.close()
+    assert res["newton-iters"] == 60 and res["status"] == _abi.ERR_NOT_CONVERGED
+    N, L = (s["N"],) * 3, (2 * s["L"],) * 3
+    P = hnc3d.Problem(N, L, s["beta"], s["rho"], s["closure"], meta["solvent"], meta["solute"], arr["chi"],
+                      s["rmax"])
+    x, its, norm = newton.jager(P.iterate_t1, np.zeros((3,) + N), 0.1, 60, 1e-14)
+    assert its == 60
+    assert np.max(np.abs(T.cpu().numpy() - x)) < 1e-10 * max(1.0, np.max(np.abs(x)))
+
+
 def test_errors_are_status_codes(fixture_loader):
     meta, arr = fixture_loader("water_hnc_n24")
     # not converged: max-iter = 1
