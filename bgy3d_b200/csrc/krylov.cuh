@@ -151,6 +151,145 @@ __global__ void k_scale_norm(long long n, T *__restrict__ w, const double *__res
     w[i] *= inv;
 }
 
+// The sweeps of the device-driven GMRES with their reductions fused in: the
+// last block to finish a sweep (an atomic ticket, reset for the next graph
+// replay) sums the block partials in a fixed order.
+//
+// k_mdot_red: h[v] = w . V_v for v < nv.
+template <typename T>
+__global__ void __launch_bounds__(256) k_mdot_red(long long nw, const T *__restrict__ w, int nv, VecSet<T> vs,
+                                                 double *__restrict__ part, unsigned *__restrict__ ticket,
+                                                 double *__restrict__ h) {
+  using VT = typename Wide<T>::type;
+  constexpr int WN = Wide<T>::n;
+  double acc[kVecMax];
+#pragma unroll
+  for (int v = 0; v < kVecMax; ++v) acc[v] = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += (long long)gridDim.x * blockDim.x) {
+    const VT a = reinterpret_cast<const VT *>(w)[i];
+    const T *ar = reinterpret_cast<const T *>(&a);
+#pragma unroll
+    for (int v = 0; v < kVecMax; ++v) {
+      if (v < nv) {
+        const VT b = reinterpret_cast<const VT *>(vs.p[v])[i];
+        const T *br = reinterpret_cast<const T *>(&b);
+        T s = T(0);
+#pragma unroll
+        for (int q = 0; q < WN; ++q) s += ar[q] * br[q];
+        acc[v] += (double)s;
+      }
+    }
+  }
+  __shared__ double sm[kVecMax][8];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int v = 0; v < kVecMax; ++v) {
+    if (v < nv) {
+      double a = acc[v];
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+      if (lane == 0) sm[v][wid] = a;
+    }
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < nv) {
+    double a = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) a += sm[threadIdx.x][q];
+    part[(long long)blockIdx.x * kVecMax + threadIdx.x] = a;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  __shared__ double red[8][kVecMax];
+  const int v = threadIdx.x % kVecMax, j = threadIdx.x / kVecMax;  // 256 threads: 8 x 32
+  double s = 0.0;
+  if (v < nv)
+    for (int b = j; b < (int)gridDim.x; b += 8) s += part[(long long)b * kVecMax + v];
+  red[j][v] = s;
+  __syncthreads();
+  if (j == 0 && v < nv) {
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) t += red[q][v];
+    h[v] = t;
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// k_maxpy_red: w -= sum_v h_v V_v (v < nv) and *hn = |w| reduced likewise.
+template <typename T>
+__global__ void __launch_bounds__(256) k_maxpy_red(long long nw, T *__restrict__ w, int nv, VecSet<T> vs,
+                                                  const double *__restrict__ h, double *__restrict__ part,
+                                                  unsigned *__restrict__ ticket, double *__restrict__ hn) {
+  using VT = typename Wide<T>::type;
+  constexpr int WN = Wide<T>::n;
+  T c[kVecMax];
+#pragma unroll
+  for (int v = 0; v < kVecMax; ++v) c[v] = (T)(v < nv ? h[v] : 0.0);
+  double s2 = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += (long long)gridDim.x * blockDim.x) {
+    const VT a = reinterpret_cast<const VT *>(w)[i];
+    const T *ar = reinterpret_cast<const T *>(&a);
+    VT o;
+    T *r = reinterpret_cast<T *>(&o);
+#pragma unroll
+    for (int q = 0; q < WN; ++q) r[q] = ar[q];
+#pragma unroll
+    for (int v = 0; v < kVecMax; ++v) {
+      if (v < nv) {
+        const VT b = reinterpret_cast<const VT *>(vs.p[v])[i];
+        const T *br = reinterpret_cast<const T *>(&b);
+#pragma unroll
+        for (int q = 0; q < WN; ++q) r[q] -= c[v] * br[q];
+      }
+    }
+    T sq = T(0);
+#pragma unroll
+    for (int q = 0; q < WN; ++q) sq += r[q] * r[q];
+    s2 += (double)sq;
+    reinterpret_cast<VT *>(w)[i] = o;
+  }
+  __shared__ double sm[8];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  if (lane == 0) sm[wid] = s2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) a += sm[q];
+    part[blockIdx.x] = a;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) s += part[b];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q = 0; q < (int)blockDim.x; ++q) t += red[q];
+    *hn = sqrt(t);
+    *ticket = 0u;
+  }
+}
+
+// w /= *hn (w = 0 when it is 0).
+template <typename T> __global__ void k_scale_by(long long n, T *__restrict__ w, const double *__restrict__ hn) {
+  const double s = *hn;
+  const T inv = s > 0.0 ? (T)(1.0 / s) : T(0);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    w[i] *= inv;
+}
+
 // Least squares of a k-step Arnoldi run, on one thread: min |beta e1 - H y|
 // with H's column j at H[j * (k + 1) + i], i <= j + 1; then y[0] += beta,
 // so that sum y_j V_j = x + r0 (the GMRES iterate plus its right-hand side).

@@ -243,6 +243,7 @@ struct rism3d_ctx {
   cudaGraph_t cg_graph = nullptr;
   cudaGraphExec_t cg_exec = nullptr;
   double *cg_H = nullptr, *cg_aux = nullptr;  // Hessenberg columns; norm, beta, y
+  unsigned *cg_ticket = nullptr;              // last-block ticket of the fused sweeps
   long long cg_nodes = 0;
   bool cg_failed = false;
 
@@ -253,6 +254,7 @@ struct rism3d_ctx {
   // shape-specialised passes: available per precision ([0] FP64, [1] FP32),
   // with TMA descriptors of W for the y and z tiles
   bool stat[2] = {false, false};
+  int zb[2] = {4, 8};  // z tile width of the shape-specialised z pass ([0] FP64, [1] FP32: 8 or 4)
   CUtensorMap tmy[2], tmz[2];
   int *d_err = nullptr;  // set by a kernel whose bounded wait timed out
 
@@ -268,7 +270,7 @@ struct rism3d_ctx {
     for (auto p : zbasis64) fr(p);
     for (auto p : zbasis32) fr(p);
     for (int a = 0; a < 3; ++a) { fr(tR[a]); fr(tRt[a]); fr(tP[a]); fr(tPt[a]); }
-    fr(tA); fr(tB); fr(tc_r); fr(tc_y); fr(cg_H); fr(cg_aux); fr(tC); fr(tD);
+    fr(tA); fr(tB); fr(tc_r); fr(tc_y); fr(cg_H); fr(cg_aux); fr(cg_ticket); fr(tC); fr(tD);
     if (cg_exec) cudaGraphExecDestroy(cg_exec);
     if (cg_graph) cudaGraphDestroy(cg_graph);
     delete coarse;
@@ -366,8 +368,8 @@ template <typename T, int M> constexpr size_t xs_smem() {
 template <typename T, int N> constexpr size_t ys_smem() {
   return sizeof(typename Cx<T>::type) * (size_t)(N * static_B<T>() + N) + 16;
 }
-template <typename T, int N> size_t zs_smem(int m) {
-  return sizeof(typename Cx<T>::type) * (size_t)(m * N * static_Bz<T>() + N) + 16;
+template <typename T, int N> size_t zs_smem(int m, int B = static_Bz<T>()) {
+  return sizeof(typename Cx<T>::type) * (size_t)(m * N * B + N) + 16;
 }
 // Lengths with shape-specialised passes: the coarse grids (48, 96) and the
 // even 2^a 3^b grids of the many-solute workloads whose two-step split fits
@@ -495,15 +497,20 @@ template <typename T, int MODE> void launch_z(rism3d_ctx *c) {
   auto *W = c->work<T>();
   const ZParams<T> zp = zparams<T>(c, MODE == MODE_F);
   if (c->stat[sizeof(T) == 8 ? 0 : 1]) {
-    constexpr int B = static_Bz<T>();
+    constexpr int BW = static_Bz<T>(), BN = static_Bz<T>() / 2;  // wide / narrow tiles
+    const int B = c->zb[sizeof(T) == 8 ? 0 : 1];
     dim3 grid((c->g.Nh + B - 1) / B, c->g.N1);
     const CUtensorMap &tm = c->tmz[sizeof(T) == 8 ? 0 : 1];
     const auto *tw = static_cast<const typename Cx<T>::type *>(c->plan<T>(2).tw);
     switch (c->g.N2) {
-#define Z_CASE(N)                                                                                        \
-  case N:                                                                                                \
-    k_z_s<T, MODE, N, B, 3><<<grid, Split<N>::R1 * B, zs_smem<T, N>(c->m), c->stream>>>(c->g, tm, tw, zp, \
-                                                                                          c->d_err);     \
+#define Z_CASE(N)                                                                                          \
+  case N:                                                                                                  \
+    if (B == BW)                                                                                           \
+      k_z_s<T, MODE, N, BW, 3><<<grid, Split<N>::R1 * BW, zs_smem<T, N>(c->m, BW), c->stream>>>(c->g, tm, tw, \
+                                                                                               zp, c->d_err); \
+    else                                                                                                   \
+      k_z_s<T, MODE, N, BN, 3><<<grid, Split<N>::R1 * BN, zs_smem<T, N>(c->m, BN), c->stream>>>(c->g, tm, tw, \
+                                                                                               zp, c->d_err); \
     break;
       Z_CASE(48) Z_CASE(64) Z_CASE(72) Z_CASE(96) Z_CASE(128) Z_CASE(144) Z_CASE(192) Z_CASE(256)
 #undef Z_CASE
@@ -826,12 +833,36 @@ long long launch_total(const rism3d_ctx *c) {
   return s;
 }
 
+// Slab width J of the y / z transfers: 32 outputs per thread for the
+// restrictions (n_out <= 64: the input is read at most twice), 16 for the
+// prolongations, 8 where the threads of a narrow slab would not fill the GPU.
 void transfer_axis(rism3d_ctx *c, int outer, int n_in, int n_out, int inner, const float *in, const float *A,
                    float *out) {
   const long long tot = (long long)outer * inner;
-  dim3 g((unsigned)((tot + tg::kAxThreads - 1) / tg::kAxThreads), (unsigned)((n_out + tg::kAxJ - 1) / tg::kAxJ));
-  tg::k_transfer_axis<<<g, tg::kAxThreads, 0, c->stream>>>(outer, n_in, n_out, inner, in, A, out);
+  const unsigned gx = (unsigned)((tot + tg::kAxThreads - 1) / tg::kAxThreads);
+  int J = n_out <= 64 ? 32 : 16;
+  while (J > 8 && (long long)gx * ((n_out + J - 1) / J) < 2 * 148) J /= 2;
+  if (J == 8 || n_in > tg::kAxMaxIn) {
+    dim3 g(gx, (unsigned)((n_out + tg::kAxJ - 1) / tg::kAxJ));
+    tg::k_transfer_axis<<<g, tg::kAxThreads, 0, c->stream>>>(outer, n_in, n_out, inner, in, A, out);
+  } else {
+    dim3 g(gx, (unsigned)((n_out + J - 1) / J));
+    const size_t sm = sizeof(float) * (size_t)n_in * J;
+    if (J == 32) tg::k_transfer_axis_j<32><<<g, tg::kAxThreads, sm, c->stream>>>(outer, n_in, n_out, inner, in, A, out);
+    else tg::k_transfer_axis_j<16><<<g, tg::kAxThreads, sm, c->stream>>>(outer, n_in, n_out, inner, in, A, out);
+  }
   CKL();
+}
+
+// CTAs of a persistent kernel: as many as fit on the device at once (256
+// threads, `smem` dynamic bytes), at most `work` (the batches to walk).
+unsigned persistent_grid(const void *fn, size_t smem, unsigned work) {
+  int dev = 0, sms = 0, per = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 256, smem));
+  const unsigned n = (unsigned)std::max(1, per) * (unsigned)std::max(1, sms);
+  return std::max(1u, std::min(n, work));
 }
 
 // x-axis transfers by FFT (twogrid_fft.cuh) where the row length has a
@@ -851,7 +882,8 @@ template <typename T> bool fx_restrict(rism3d_ctx *c, long long rows, const T *i
   case M: {                                                                                                    \
     const size_t sm = fx_smem_restrict<M, kFxRX>(K, c->Nc[0]);                                                           \
     if (sm > 48 * 1024) return false;                                                                         \
-    k_restrict_fx<T, M, kFxRX><<<nb, 256, sm, c->stream>>>(rows, c->Nc[0], K, in, (float)s, post, tw, c->tC, c->tA); \
+    k_restrict_fx<T, M, kFxRX><<<persistent_grid((const void *)k_restrict_fx<T, M, kFxRX>, sm, nb), 256, sm,     \
+                                 c->stream>>>(rows, c->Nc[0], K, in, (float)s, post, tw, c->tC, c->tA);           \
     break;                                                                                                     \
   }
     FXR(24) FXR(32) FXR(36) FXR(48) FXR(64) FXR(72) FXR(96) FXR(128)
@@ -872,7 +904,8 @@ template <typename T> bool fx_prolong(rism3d_ctx *c, long long rows, const T *r,
   case M: {                                                                                                    \
     const size_t sm = fx_smem_prolong<M, kFxRX>(K, c->Nc[0]);                                                  \
     if (sm > 48 * 1024) return false;                                                                         \
-    k_prolong_fx<T, T, M, kFxRX><<<nb, 256, sm, c->stream>>>(rows, c->Nc[0], K, c->tA, post, tw, c->tD, r, s, out); \
+    k_prolong_fx<T, T, M, kFxRX><<<persistent_grid((const void *)k_prolong_fx<T, T, M, kFxRX>, sm, nb), 256, sm,  \
+                                   c->stream>>>(rows, c->Nc[0], K, c->tA, post, tw, c->tD, r, s, out);            \
     break;                                                                                                     \
   }
     FXP(24) FXP(32) FXP(36) FXP(48) FXP(64) FXP(72) FXP(96) FXP(128)
@@ -917,7 +950,7 @@ template <typename T> void tg_prepare(rism3d_ctx *c, const T *d) {
 }
 
 int coarse_steps(const rism3d_ctx *c) {
-  return c->pd.coarse_steps > 0 ? std::min(c->pd.coarse_steps, kVecMax - 1) : 12;
+  return c->pd.coarse_steps > 0 ? std::min(c->pd.coarse_steps, kVecMax - 1) : 16;
 }
 
 // The coarse solve driven entirely on the device: k GMRES steps from zero
@@ -946,11 +979,10 @@ void coarse_solve_dev(rism3d_ctx *c, int k) {
     VecSet<float> vs{};
     for (int i = 0; i < kVecMax; ++i) vs.p[i] = B[i <= j ? i : 0];
     double *h = H + (size_t)j * (k + 1);
-    k_mdotv<float><<<G, 256, 0, st>>>(nw, B[j + 1], j + 1, vs, cc->dpart);
-    k_colsum<<<1, kVecMax * 8, 0, st>>>(G, kVecMax, j + 1, cc->dpart, h);
-    k_maxpyv<float><<<G, 256, 0, st>>>(nw, B[j + 1], 1.0, j + 1, vs, one, h, cc->dpart);
-    k_colsum<<<1, kVecMax * 8, 0, st>>>(G, 1, 1, cc->dpart, nrm);
-    k_scale_norm<float><<<gv, 256, 0, st>>>(cc->nvec, B[j + 1], nrm, h + j + 1);
+    // classical Gram-Schmidt, each sweep with its reduction fused in
+    k_mdot_red<float><<<G, 256, 0, st>>>(nw, B[j + 1], j + 1, vs, cc->dpart, c->cg_ticket, h);
+    k_maxpy_red<float><<<G, 256, 0, st>>>(nw, B[j + 1], j + 1, vs, h, cc->dpart, c->cg_ticket, h + j + 1);
+    k_scale_by<float><<<gv, 256, 0, st>>>(cc->nvec, B[j + 1], h + j + 1);
     CKL();
   }
   k_arnoldi_lsq<<<1, 1, 0, st>>>(k, H, beta, y);
@@ -976,6 +1008,10 @@ bool coarse_graph(rism3d_ctx *c, int k) {
   slopebuf<float>(cc);
   if (!c->cg_H) c->cg_H = dalloc<double>((size_t)k * (k + 1));
   if (!c->cg_aux) c->cg_aux = dalloc<double>((size_t)k + 2);
+  if (!c->cg_ticket) {
+    c->cg_ticket = dalloc<unsigned>(1);
+    CK(cudaMemsetAsync(c->cg_ticket, 0, sizeof(unsigned), c->stream));
+  }
   cudaStream_t cap = nullptr;
   CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
   cudaStream_t saved = cc->stream;
@@ -1637,6 +1673,7 @@ void bind_solute(rism3d_ctx *c, int n, const rism3d_site *solute) {
 struct TuneVal {
   TileShape t[2];
   bool stat[2];
+  int zb[2];
 };
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int, int>, TuneVal> g_tune;
@@ -1698,7 +1735,7 @@ template <typename T> void tune_precision(rism3d_ctx *c, const T *A, const T *Bv
       const int keep = *fields[axis];
       *fields[axis] = k;
       const float ms = time_ms(c, run, reps);
-      if (ms < best_ms) { best_ms = ms; best = k; }
+      if (ms < 0.97f * best_ms) { best_ms = ms; best = k; }  // a clear win only: timings are noisy
       *fields[axis] = keep;
     }
     *fields[axis] = best;
@@ -1706,8 +1743,23 @@ template <typename T> void tune_precision(rism3d_ctx *c, const T *A, const T *Bv
   if (had_stat) {
     const float g_ms = time_ms(c, run, reps);
     c->stat[pr] = true;
-    const float s_ms = time_ms(c, run, reps);
-    c->stat[pr] = s_ms <= g_ms;
+    float s_ms = time_ms(c, run, reps);
+    // the specialised z pass: wide tiles, or half as wide (twice the CTAs
+    // in flight per SM)
+    const int wide = c->zb[pr];
+    float n_ms = 1e30f;
+    if (pr == 1) {  // FP32 only: 64-byte rows (FP64 would drop to 32-thread CTAs)
+      c->zb[pr] = wide / 2;
+      make_tmap(c, &c->tmz[pr], pr == 0, c->zb[pr], 1, G.N2);
+      n_ms = time_ms(c, run, reps);
+    }
+    if (n_ms < 0.95f * s_ms) {
+      s_ms = n_ms;
+    } else {
+      c->zb[pr] = wide;
+      make_tmap(c, &c->tmz[pr], pr == 0, wide, 1, G.N2);
+    }
+    c->stat[pr] = s_ms <= 1.05f * g_ms;  // keep the specialised passes unless clearly slower
   }
 }
 
@@ -1725,6 +1777,10 @@ void autotune(rism3d_ctx *c) {
       for (int pr = 0; pr < 2; ++pr) {
         c->tiles[pr] = it->second.t[pr];
         c->stat[pr] = c->stat[pr] && it->second.stat[pr];
+        if (c->stat[pr] && c->zb[pr] != it->second.zb[pr]) {
+          c->zb[pr] = it->second.zb[pr];
+          make_tmap(c, &c->tmz[pr], pr == 0, c->zb[pr], 1, G.N2);
+        }
       }
       return;
     }
@@ -1748,6 +1804,7 @@ void autotune(rism3d_ctx *c) {
   for (int pr = 0; pr < 2; ++pr) {
     v.t[pr] = c->tiles[pr];
     v.stat[pr] = c->stat[pr];
+    v.zb[pr] = c->zb[pr];
   }
   g_tune[key] = v;
 }
@@ -1838,7 +1895,7 @@ void init_work(rism3d_ctx *c) {
   c->W = dalloc<double2>((size_t)G.m * G.Nc);
   // reduction blocks: about four 16-byte loads per thread, at most 4 per SM
   c->red_blocks = (int)std::min<long long>(592, std::max<long long>(8, (c->nvec / 4 + 1023) / 1024));
-  c->dpart = dalloc<double>((size_t)c->red_blocks * kVecMax + 64);
+  c->dpart = dalloc<double>((size_t)c->red_blocks * (kVecMax + 1) + 64);
   c->dres = dalloc<double>(4 * kVecMax);
   const int rows = G.N1 * G.N2;
   // partials for the smallest x batch the tile autotuner may pick
@@ -2004,9 +2061,8 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
         !(gen && gen[0] == '1')) {
       for (int pr = 0; pr < 2; ++pr) {
         const int B = pr == 0 ? static_B<double>() : static_B<float>();
-        const int Bz = pr == 0 ? static_Bz<double>() : static_Bz<float>();
         make_tmap(c, &c->tmy[pr], pr == 0, B, G.N1, 1);
-        make_tmap(c, &c->tmz[pr], pr == 0, Bz, 1, G.N2);
+        make_tmap(c, &c->tmz[pr], pr == 0, c->zb[pr], 1, G.N2);
         c->stat[pr] = true;
       }
     }
@@ -2085,7 +2141,23 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
   allow((const void *)k_y_s<T, false, 256, static_B<T>()>);      \
   allow((const void *)k_y_s<T, true, 256, static_B<T>()>);       \
   allow((const void *)k_z_s<T, MODE_F, 256, static_Bz<T>(), 3>); \
-  allow((const void *)k_z_s<T, MODE_J, 256, static_Bz<T>(), 3>);
+  allow((const void *)k_z_s<T, MODE_J, 256, static_Bz<T>(), 3>); \
+  allow((const void *)k_z_s<T, MODE_F, 48, static_Bz<T>() / 2, 3>);  \
+  allow((const void *)k_z_s<T, MODE_J, 48, static_Bz<T>() / 2, 3>);  \
+  allow((const void *)k_z_s<T, MODE_F, 64, static_Bz<T>() / 2, 3>);  \
+  allow((const void *)k_z_s<T, MODE_J, 64, static_Bz<T>() / 2, 3>);  \
+  allow((const void *)k_z_s<T, MODE_F, 72, static_Bz<T>() / 2, 3>);  \
+  allow((const void *)k_z_s<T, MODE_J, 72, static_Bz<T>() / 2, 3>);  \
+  allow((const void *)k_z_s<T, MODE_F, 96, static_Bz<T>() / 2, 3>);  \
+  allow((const void *)k_z_s<T, MODE_J, 96, static_Bz<T>() / 2, 3>);  \
+  allow((const void *)k_z_s<T, MODE_F, 128, static_Bz<T>() / 2, 3>); \
+  allow((const void *)k_z_s<T, MODE_J, 128, static_Bz<T>() / 2, 3>); \
+  allow((const void *)k_z_s<T, MODE_F, 144, static_Bz<T>() / 2, 3>); \
+  allow((const void *)k_z_s<T, MODE_J, 144, static_Bz<T>() / 2, 3>); \
+  allow((const void *)k_z_s<T, MODE_F, 192, static_Bz<T>() / 2, 3>); \
+  allow((const void *)k_z_s<T, MODE_J, 192, static_Bz<T>() / 2, 3>); \
+  allow((const void *)k_z_s<T, MODE_F, 256, static_Bz<T>() / 2, 3>); \
+  allow((const void *)k_z_s<T, MODE_J, 256, static_Bz<T>() / 2, 3>);
       OPTIN_S(double)
       OPTIN_S(float)
 #undef OPTIN_S
@@ -2166,6 +2238,8 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
           CK(cudaMemcpy(c->tC, Ct.data(), sizeof(float2) * Ct.size(), cudaMemcpyHostToDevice));
           CK(cudaMemcpy(c->tD, Dt.data(), sizeof(float2) * Dt.size(), cudaMemcpyHostToDevice));
         }
+        allow_smem((const void *)tg::k_transfer_axis_j<32>, sizeof(float) * tg::kAxMaxIn * 32);
+        allow_smem((const void *)tg::k_transfer_axis_j<16>, sizeof(float) * tg::kAxMaxIn * 16);
         c->tA = dalloc<float>((size_t)m * G.N2 * G.N1 * c->Nc[0]);
         c->tB = dalloc<float>((size_t)m * G.N2 * c->Nc[1] * c->Nc[0]);
         c->tc_r = dalloc<float>(c->coarse->nvec);
@@ -2579,7 +2653,7 @@ void rism3d_problem_defaults(rism3d_problem *pd, double L_half, int N) {
   pd->krylov_restart = 30;
   pd->ew_forcing = 1;
   pd->coarse_h = 0.75;
-  pd->coarse_steps = 12;
+  pd->coarse_steps = 16;
 }
 
 const char *rism3d_last_error(void) { return g_last_error.c_str(); }
@@ -2694,6 +2768,7 @@ int rism3d_tile_shapes(rism3d_ctx *ctx, int *out) {
     out[3 * pr + 1] = ctx->tiles[pr].BY;
     out[3 * pr + 2] = ctx->tiles[pr].BZ;
     out[6 + pr] = ctx->stat[pr] ? 1 : 0;
+    out[8 + pr] = ctx->zb[pr];
   }
   return RISM3D_OK;
 }

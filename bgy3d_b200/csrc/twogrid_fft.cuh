@@ -57,6 +57,9 @@ template <> struct Quad<double> {
 
 // out[row][i] (rows x Nc, FP32) = restriction of s * in[row][.] (rows x 2M).
 // ctab[k][i] = c_k e^{2 pi i k i / Nc} / N0, c = 1, 2, ..., 2, 1.
+// Persistent: each CTA stages the twiddles and the table once and walks
+// batches of RX rows with stride gridDim.x; the next batch's rows are loaded
+// into registers while the current one is transformed.
 template <typename TI, int M, int RX>
 __global__ void __launch_bounds__(256) k_restrict_fx(long long rows, int Nc, int K, const TI *__restrict__ in,
                                                      float s, const float2 *__restrict__ post,
@@ -73,58 +76,70 @@ __global__ void __launch_bounds__(256) k_restrict_fx(long long rows, int Nc, int
   const int K1 = K + 1;
   V *X = C + K1 * Nc;
   const int tid = threadIdx.x;
-  const long long row0 = (long long)blockIdx.x * RX;
-  // all row loads in flight before any use
+  const long long nbat = (rows + RX - 1) / RX;
+  long long bat = blockIdx.x;
   Q ra[CNT];
-#pragma unroll
-  for (int it = 0; it < CNT; ++it) {
-    const int e = tid + it * 256;
-    const int row = e / PER, jj = (e % PER) * 2;
-    if (e < RX * PER && row0 + row < rows) ra[it] = *reinterpret_cast<const Q *>(in + (row0 + row) * N0 + 2 * jj);
+#define FX_LOAD_ROWS(BAT)                                                                           \
+  {                                                                                                 \
+    const long long r0 = (BAT) * RX;                                                                \
+    _Pragma("unroll") for (int it = 0; it < CNT; ++it) {                                            \
+      const int e = tid + it * 256;                                                                 \
+      const int row = e / PER, jj = (e % PER) * 2;                                                  \
+      if (e < RX * PER && r0 + row < rows) ra[it] = *reinterpret_cast<const Q *>(in + (r0 + row) * N0 + 2 * jj); \
+    }                                                                                               \
   }
+  if (bat < nbat) FX_LOAD_ROWS(bat)
   for (int q = tid; q < M; q += 256) tw[q] = twg[q];
   for (int q = tid; q < K1 * Nc; q += 256) C[q] = ctab[q];
+  for (; bat < nbat; bat += gridDim.x) {
+    const long long row0 = bat * RX;
 #pragma unroll
-  for (int it = 0; it < CNT; ++it) {
-    const int e = tid + it * 256;
-    if (e >= RX * PER) break;
-    const int row = e / PER, jj = (e % PER) * 2;
-    V a = make_float2(0.f, 0.f), b = a;
-    if (row0 + row < rows) {
-      Quad<TI>::split(ra[it], a, b);
-      a.x *= s; a.y *= s; b.x *= s; b.y *= s;
+    for (int it = 0; it < CNT; ++it) {
+      const int e = tid + it * 256;
+      if (e >= RX * PER) break;
+      const int row = e / PER, jj = (e % PER) * 2;
+      V a = make_float2(0.f, 0.f), b = a;
+      if (row0 + row < rows) {
+        Quad<TI>::split(ra[it], a, b);
+        a.x *= s; a.y *= s; b.x *= s; b.y *= s;
+      }
+      buf[Lay::at(jj, row)] = a;
+      buf[Lay::at(jj + 1, row)] = b;
     }
-    buf[Lay::at(jj, row)] = a;
-    buf[Lay::at(jj + 1, row)] = b;
-  }
-  __syncthreads();
-  fft2<M, RX, 256, false, false, Lay>(buf, tw);
-  for (int e = tid; e < RX * K1; e += 256) {
-    const int row = e / K1, k = e - row * K1;
-    const V zk = buf[Lay::at(k, row)];
-    const V zm = buf[Lay::at(k == 0 ? 0 : M - k, row)];
-    V E, O;
-    E.x = (zk.x + zm.x) * 0.5f;
-    E.y = (zk.y - zm.y) * 0.5f;
-    O.x = (zk.y + zm.y) * 0.5f;
-    O.y = -(zk.x - zm.x) * 0.5f;
-    X[row * K1 + k] = cadd(E, cmul(post[k], O));
-  }
-  __syncthreads();
-  for (int e = tid; e < RX * Nc; e += 256) {
-    const int row = e / Nc, i = e - row * Nc;
-    if (row0 + row >= rows) continue;
-    float acc = 0.f;
-    for (int k = 0; k < K1; ++k) {
-      const V c = C[k * Nc + i], x = X[row * K1 + k];
-      acc = fmaf(c.x, x.x, fmaf(-c.y, x.y, acc));
+    if (bat + gridDim.x < nbat) FX_LOAD_ROWS(bat + gridDim.x)
+    __syncthreads();
+    fft2<M, RX, 256, false, false, Lay>(buf, tw);
+    for (int e = tid; e < RX * K1; e += 256) {
+      const int row = e / K1, k = e - row * K1;
+      const V zk = buf[Lay::at(k, row)];
+      const V zm = buf[Lay::at(k == 0 ? 0 : M - k, row)];
+      V E, O;
+      E.x = (zk.x + zm.x) * 0.5f;
+      E.y = (zk.y - zm.y) * 0.5f;
+      O.x = (zk.y + zm.y) * 0.5f;
+      O.y = -(zk.x - zm.x) * 0.5f;
+      X[row * K1 + k] = cadd(E, cmul(post[k], O));
     }
-    out[(row0 + row) * Nc + i] = acc;
+    __syncthreads();
+    for (int e = tid; e < RX * Nc; e += 256) {
+      const int row = e / Nc, i = e - row * Nc;
+      if (row0 + row >= rows) continue;
+      float acc = 0.f;
+      for (int k = 0; k < K1; ++k) {
+        const V c = C[k * Nc + i], x = X[row * K1 + k];
+        acc = fmaf(c.x, x.x, fmaf(-c.y, x.y, acc));
+      }
+      out[(row0 + row) * Nc + i] = acc;
+    }
+    __syncthreads();
   }
+#undef FX_LOAD_ROWS
 }
 
 // out[row][j] (rows x 2M) = prolongation of y[row][.] (rows x Nc, FP32) - s r.
-// dtab[i][k] = f_k e^{-2 pi i k i / Nc} (k fastest).
+// dtab[i][k] = f_k e^{-2 pi i k i / Nc} (k fastest).  Persistent as
+// k_restrict_fx: the next batch's coarse rows and subtracted fine rows are
+// in flight while the current batch is transformed.
 template <typename TO, typename TR, int M, int RX>
 __global__ void __launch_bounds__(256) k_prolong_fx(long long rows, int Nc, int K, const float *__restrict__ y,
                                                     const float2 *__restrict__ post, const float2 *__restrict__ twg,
@@ -142,74 +157,99 @@ __global__ void __launch_bounds__(256) k_prolong_fx(long long rows, int Nc, int 
   V *X = D + K1 * Nc;
   float *ys = reinterpret_cast<float *>(X + RX * K1);
   const int tid = threadIdx.x;
-  const long long row0 = (long long)blockIdx.x * RX;
-  // the subtracted rows are fetched first; their latency hides behind the work
-  QR rr[CNT];
-#pragma unroll
-  for (int it = 0; it < CNT; ++it) {
-    const int e = tid + it * 256;
-    const int row = e / PER, jj = (e % PER) * 2;
-    if (e < RX * PER && row0 + row < rows) rr[it] = *reinterpret_cast<const QR *>(r + (row0 + row) * N0 + 2 * jj);
+  const long long nbat = (rows + RX - 1) / RX;
+  const int YC = (RX * Nc + 255) / 256;  // coarse values per thread; Nc < 2M <= 256 keeps it <= RX
+  long long bat = blockIdx.x;
+  QR rr[CNT], rn[CNT];
+  float yv[RX];
+#define FX_LOAD(BAT, RR)                                                                            \
+  {                                                                                                 \
+    const long long r0 = (BAT) * RX;                                                                \
+    _Pragma("unroll") for (int it = 0; it < CNT; ++it) {                                            \
+      const int e = tid + it * 256;                                                                 \
+      const int row = e / PER, jj = (e % PER) * 2;                                                  \
+      if (e < RX * PER && r0 + row < rows) RR[it] = *reinterpret_cast<const QR *>(r + (r0 + row) * N0 + 2 * jj); \
+    }                                                                                               \
+    _Pragma("unroll") for (int q = 0; q < RX; ++q) {                                                \
+      const int e = tid + q * 256;                                                                  \
+      if (q < YC) yv[q] = (e < RX * Nc && r0 + e / Nc < rows) ? y[r0 * Nc + e] : 0.f;               \
+    }                                                                                               \
   }
+  if (bat < nbat) FX_LOAD(bat, rr)
   for (int q = tid; q < M; q += 256) tw[q] = twg[q];
   for (int q = tid; q < K1 * Nc; q += 256) D[q] = dtab[q];
-  for (int e = tid; e < RX * Nc; e += 256) ys[e] = (row0 + e / Nc < rows) ? y[row0 * Nc + e] : 0.f;
-  __syncthreads();
-  for (int e = tid; e < RX * K1; e += 256) {
-    const int row = e / K1, k = e - row * K1;
-    float ax = 0.f, ay = 0.f;
-    for (int i = 0; i < Nc; ++i) {
-      const V d = D[i * K1 + k];
-      const float v = ys[row * Nc + i];
-      ax = fmaf(d.x, v, ax);
-      ay = fmaf(d.y, v, ay);
-    }
-    X[row * K1 + k] = make_float2(ax, ay);
-  }
-  __syncthreads();
-  for (int e = tid; e < RX * H; e += 256) {
-    const int row = e / H, k = e - row * H;
-    V xk = make_float2(0.f, 0.f), xm = make_float2(0.f, 0.f);
-    if (k <= K) xk = X[row * K1 + k];
-    if (M - k <= K) xm = X[row * K1 + (M - k)];
-    if (k == 0) { xk.y = 0.f; xm.y = 0.f; }
-    V Aa, Dd;
-    Aa.x = xk.x + xm.x; Aa.y = xk.y - xm.y;
-    Dd.x = xk.x - xm.x; Dd.y = xk.y + xm.y;
-    const V Pp = cmul(Dd, cconj(post[k]));
-    V zk, zm;
-    zk.x = Aa.x - Pp.y; zk.y = Aa.y + Pp.x;
-    zm.x = Aa.x + Pp.y; zm.y = -(Aa.y - Pp.x);
-    buf[Lay::at(k, row)] = zk;
-    if (k != 0 && M - k != k) buf[Lay::at(M - k, row)] = zm;
-  }
-  __syncthreads();
-  fft2<M, RX, 256, true, false, Lay>(buf, tw);
+  for (; bat < nbat; bat += gridDim.x) {
+    const long long row0 = bat * RX;
 #pragma unroll
-  for (int it = 0; it < CNT; ++it) {
-    const int e = tid + it * 256;
-    if (e >= RX * PER) break;
-    const int row = e / PER, jj = (e % PER) * 2;
-    if (row0 + row >= rows) continue;
-    V ra, rb;
-    Quad<TR>::split(rr[it], ra, rb);
-    const V za = buf[Lay::at(jj, row)], zb = buf[Lay::at(jj + 1, row)];
-    TO *o = out + (row0 + row) * N0 + 2 * jj;
-    // the subtracted term in the output precision (r kept exact for FP64)
-    const TR *rx = r + (row0 + row) * N0 + 2 * jj;
-    if (sizeof(TR) == 8) {
-      o[0] = (TO)((double)za.x - s * (double)rx[0]);
-      o[1] = (TO)((double)za.y - s * (double)rx[1]);
-      o[2] = (TO)((double)zb.x - s * (double)rx[2]);
-      o[3] = (TO)((double)zb.y - s * (double)rx[3]);
-    } else {
-      const float sf = (float)s;
-      o[0] = (TO)(za.x - sf * ra.x);
-      o[1] = (TO)(za.y - sf * ra.y);
-      o[2] = (TO)(zb.x - sf * rb.x);
-      o[3] = (TO)(zb.y - sf * rb.y);
+    for (int q = 0; q < RX; ++q) {
+      const int e = tid + q * 256;
+      if (q < YC && e < RX * Nc) ys[e] = yv[q];
     }
+    const bool more = bat + gridDim.x < nbat;
+    if (more) FX_LOAD(bat + gridDim.x, rn)
+    __syncthreads();
+    for (int e = tid; e < RX * K1; e += 256) {
+      const int row = e / K1, k = e - row * K1;
+      float ax = 0.f, ay = 0.f;
+      for (int i = 0; i < Nc; ++i) {
+        const V d = D[i * K1 + k];
+        const float v = ys[row * Nc + i];
+        ax = fmaf(d.x, v, ax);
+        ay = fmaf(d.y, v, ay);
+      }
+      X[row * K1 + k] = make_float2(ax, ay);
+    }
+    __syncthreads();
+    for (int e = tid; e < RX * H; e += 256) {
+      const int row = e / H, k = e - row * H;
+      V xk = make_float2(0.f, 0.f), xm = make_float2(0.f, 0.f);
+      if (k <= K) xk = X[row * K1 + k];
+      if (M - k <= K) xm = X[row * K1 + (M - k)];
+      if (k == 0) { xk.y = 0.f; xm.y = 0.f; }
+      V Aa, Dd;
+      Aa.x = xk.x + xm.x; Aa.y = xk.y - xm.y;
+      Dd.x = xk.x - xm.x; Dd.y = xk.y + xm.y;
+      const V Pp = cmul(Dd, cconj(post[k]));
+      V zk, zm;
+      zk.x = Aa.x - Pp.y; zk.y = Aa.y + Pp.x;
+      zm.x = Aa.x + Pp.y; zm.y = -(Aa.y - Pp.x);
+      buf[Lay::at(k, row)] = zk;
+      if (k != 0 && M - k != k) buf[Lay::at(M - k, row)] = zm;
+    }
+    __syncthreads();
+    fft2<M, RX, 256, true, false, Lay>(buf, tw);
+#pragma unroll
+    for (int it = 0; it < CNT; ++it) {
+      const int e = tid + it * 256;
+      if (e >= RX * PER) break;
+      const int row = e / PER, jj = (e % PER) * 2;
+      if (row0 + row >= rows) continue;
+      V ra, rb;
+      Quad<TR>::split(rr[it], ra, rb);
+      const V za = buf[Lay::at(jj, row)], zb = buf[Lay::at(jj + 1, row)];
+      TO *o = out + (row0 + row) * N0 + 2 * jj;
+      // the subtracted term in the output precision (r kept exact for FP64)
+      const TR *rx = r + (row0 + row) * N0 + 2 * jj;
+      if (sizeof(TR) == 8) {
+        o[0] = (TO)((double)za.x - s * (double)rx[0]);
+        o[1] = (TO)((double)za.y - s * (double)rx[1]);
+        o[2] = (TO)((double)zb.x - s * (double)rx[2]);
+        o[3] = (TO)((double)zb.y - s * (double)rx[3]);
+      } else {
+        const float sf = (float)s;
+        o[0] = (TO)(za.x - sf * ra.x);
+        o[1] = (TO)(za.y - sf * ra.y);
+        o[2] = (TO)(zb.x - sf * rb.x);
+        o[3] = (TO)(zb.y - sf * rb.y);
+      }
+    }
+    if (more) {
+#pragma unroll
+      for (int it = 0; it < CNT; ++it) rr[it] = rn[it];
+    }
+    __syncthreads();
   }
+#undef FX_LOAD
 }
 
 }  // namespace rism

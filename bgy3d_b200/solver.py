@@ -28,7 +28,7 @@ DEFAULTS = {
     # forcing (0: the reference's fixed rtol 1e-3), the two-grid
     # preconditioner's coarse spacing in A (0: off, the reference's
     # unpreconditioned GMRES) and its coarse GMRES steps.
-    "krylov-restart": 30, "ew-forcing": 1, "coarse-h": 0.75, "coarse-steps": 12,
+    "krylov-restart": 30, "ew-forcing": 1, "coarse-h": 0.75, "coarse-steps": 16,
 }
 
 
@@ -378,10 +378,11 @@ class RismContext:
 
     def tile_shapes(self):
         """The pass schedule chosen at creation (rism3d_tile_shapes):
-        {"f64": (RX, BY, BZ, shape-specialised), "f32": (...)}."""
-        out = (ctypes.c_int * 8)()
+        {"f64": (RX, BY, BZ, shape-specialised, its z width), "f32": (...)}."""
+        out = (ctypes.c_int * 10)()
         _abi.check(_abi.lib().rism3d_tile_shapes(self._h, out), "rism3d_tile_shapes")
-        return {"f64": (out[0], out[1], out[2], bool(out[6])), "f32": (out[3], out[4], out[5], bool(out[7]))}
+        return {"f64": (out[0], out[1], out[2], bool(out[6]), out[8]),
+                "f32": (out[3], out[4], out[5], bool(out[7]), out[9])}
 
     def coarse_grid(self):
         """Points per axis of the two-grid preconditioner's coarse grid

@@ -96,7 +96,7 @@ typedef struct rism3d_problem {
                          used when n <= N/2 on every axis; otherwise the
                          grid of max(coarse_h, 1 A) spacing if it is coarser
                          than N on every axis; off when 0 or neither fits */
-  int coarse_steps;   /* GMRES steps of each coarse solve (0: 12) */
+  int coarse_steps;   /* GMRES steps of each coarse solve (0: 16; defaults: 16) */
 } rism3d_problem;
 
 /* What hnc3d_solute_solve conses onto its result alist
@@ -289,10 +289,11 @@ int rism3d_gradient(rism3d_ctx *ctx, const double *T, rism3d_grad *grad);
    seconds = device time.  PY has no closure differential: RISM3D_ERR_UNSUPPORTED. */
 int rism3d_response(rism3d_ctx *ctx, const double *T, rism3d_grad *grad);
 
-/* The pass schedule the context runs, written to out[8]: x rows, y and z
+/* The pass schedule the context runs, written to out[10]: x rows, y and z
    columns per CTA of the runtime-length passes for FP64 (out[0..2]) and
-   FP32 (out[3..5]), and whether the shape-specialised passes run (out[6]
-   FP64, out[7] FP32).  Chosen when the context is created by timing the
+   FP32 (out[3..5]), whether the shape-specialised passes run (out[6]
+   FP64, out[7] FP32) and the z-column width of their z pass (out[8],
+   out[9]).  Chosen when the context is created by timing the
    candidates on its own buffers, once per grid shape and process
    (RISM3D_AUTOTUNE=0: a register / occupancy rule instead). */
 int rism3d_tile_shapes(rism3d_ctx *ctx, int *out);
