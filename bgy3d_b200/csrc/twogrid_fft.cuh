@@ -121,15 +121,31 @@ __global__ void __launch_bounds__(256) k_restrict_fx(long long rows, int Nc, int
       X[row * K1 + k] = cadd(E, cmul(post[k], O));
     }
     __syncthreads();
-    for (int e = tid; e < RX * Nc; e += 256) {
-      const int row = e / Nc, i = e - row * Nc;
-      if (row0 + row >= rows) continue;
-      float acc = 0.f;
-      for (int k = 0; k < K1; ++k) {
-        const V c = C[k * Nc + i], x = X[row * K1 + k];
-        acc = fmaf(c.x, x.x, fmaf(-c.y, x.y, acc));
+    // (K+1) x Nc table product, register-blocked 2 rows x 4 outputs per
+    // thread: 6 shared loads per 8 complex products (shared-memory bandwidth
+    // bounds this loop)
+    {
+      const int NQ = (Nc + 3) / 4;
+      for (int e = tid; e < (RX / 2) * NQ; e += 256) {
+        const int r2 = (e / NQ) * 2, i0 = (e % NQ) * 4;
+        float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+        for (int k = 0; k < K1; ++k) {
+          const V x0 = X[r2 * K1 + k], x1 = X[(r2 + 1) * K1 + k];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const V c = i0 + q < Nc ? C[k * Nc + i0 + q] : make_float2(0.f, 0.f);
+            acc[0][q] = fmaf(c.x, x0.x, fmaf(-c.y, x0.y, acc[0][q]));
+            acc[1][q] = fmaf(c.x, x1.x, fmaf(-c.y, x1.y, acc[1][q]));
+          }
+        }
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+          if (row0 + r2 + rr >= rows) continue;
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (i0 + q < Nc) out[(row0 + r2 + rr) * Nc + i0 + q] = acc[rr][q];
+        }
       }
-      out[(row0 + row) * Nc + i] = acc;
     }
     __syncthreads();
   }
@@ -188,16 +204,30 @@ __global__ void __launch_bounds__(256) k_prolong_fx(long long rows, int Nc, int 
     const bool more = bat + gridDim.x < nbat;
     if (more) FX_LOAD(bat + gridDim.x, rn)
     __syncthreads();
-    for (int e = tid; e < RX * K1; e += 256) {
-      const int row = e / K1, k = e - row * K1;
-      float ax = 0.f, ay = 0.f;
-      for (int i = 0; i < Nc; ++i) {
-        const V d = D[i * K1 + k];
-        const float v = ys[row * Nc + i];
-        ax = fmaf(d.x, v, ax);
-        ay = fmaf(d.y, v, ay);
+    // Nc x (K+1) table product, register-blocked 2 rows x 3 coefficients
+    // per thread: 5 shared loads per 6 complex products
+    {
+      const int KQ = (K1 + 2) / 3;
+      for (int e = tid; e < (RX / 2) * KQ; e += 256) {
+        const int r2 = (e / KQ) * 2, k0 = (e % KQ) * 3;
+        float ax[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}}, ay[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+        for (int i = 0; i < Nc; ++i) {
+          const float v0 = ys[r2 * Nc + i], v1 = ys[(r2 + 1) * Nc + i];
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            const V d = k0 + q < K1 ? D[i * K1 + k0 + q] : make_float2(0.f, 0.f);
+            ax[0][q] = fmaf(d.x, v0, ax[0][q]);
+            ay[0][q] = fmaf(d.y, v0, ay[0][q]);
+            ax[1][q] = fmaf(d.x, v1, ax[1][q]);
+            ay[1][q] = fmaf(d.y, v1, ay[1][q]);
+          }
+        }
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr)
+#pragma unroll
+          for (int q = 0; q < 3; ++q)
+            if (k0 + q < K1) X[(r2 + rr) * K1 + k0 + q] = make_float2(ax[rr][q], ay[rr][q]);
       }
-      X[row * K1 + k] = make_float2(ax, ay);
     }
     __syncthreads();
     for (int e = tid; e < RX * H; e += 256) {
