@@ -225,36 +225,18 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_y_s(Geo g, const __grid_co
   }
 }
 
-// z pass: the m [N][B] tiles of one (ky, kx-block) by TMA, forward transform,
-// OZ contraction (+ long-range terms in MODE_F), inverse transform, TMA out.
-// tm: W as {2 Nhp, N1, m N2} scalars, box {2B, 1, N2}.
+// One z tile in shared memory: forward transform along z of the m [N][B]
+// site columns, the OZ contraction with the radial chi-1 tables (+ the
+// long-range terms in MODE_F), inverse transform; ends after a barrier.
 template <typename T, int MODE, int N, int B, int MS>
-__global__ void __launch_bounds__(Split<N>::R1 * B) k_z_s(Geo g, const __grid_constant__ CUtensorMap tm,
-                                                         const typename Cx<T>::type *__restrict__ twg,
-                                                         ZParams<T> zp, int *__restrict__ err) {
+__device__ __forceinline__ void z_tile(const Geo &g, typename Cx<T>::type *buf, const typename Cx<T>::type *tw,
+                                       const ZParams<T> &zp, int kx0, int y) {
   using V = typename Cx<T>::type;
   using P2 = typename Vec2<T>::type;
   constexpr int NTHR = Split<N>::R1 * B;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int m = g.m;
-  V *buf = reinterpret_cast<V *>(smem_raw);
-  V *tw = buf + m * N * B;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(tw + N);
   const int tid = threadIdx.x;
-  const int kx0 = blockIdx.x * B, y = blockIdx.y;
   const int bw = min(B, g.Nh - kx0);
-  if (tid == 0) mbar_init(bar, 1);
-  __syncthreads();
-  if (tid == 0) {
-    mbar_expect_tx(bar, (uint32_t)(m * N * B * sizeof(V)));
-    for (int s = 0; s < m; ++s) tma_load_3d(buf + s * N * B, &tm, bar, 2 * kx0, y, s * g.N2);
-  }
-  for (int q = tid; q < N; q += NTHR) tw[q] = twg[q];
-  if (!mbar_wait(bar, 0, kMbarPolls)) {
-    if (tid == 0) atomicExch(err, 2);
-    return;
-  }
-  __syncthreads();
   for (int s = 0; s < m; ++s) fft2<N, B, NTHR, false, true, LayCol<N, B>>(buf + s * N * B, tw);
   const int ky = kfreq(y, g.N1);
   const double k1 = ky * g.dk1;
@@ -330,6 +312,37 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_z_s(Geo g, const __grid_co
   }
   __syncthreads();
   for (int s = 0; s < m; ++s) fft2<N, B, NTHR, true, true, LayCol<N, B>>(buf + s * N * B, tw);
+}
+
+// z pass: the m [N][B] tiles of one (ky, kx-block) by TMA, forward transform,
+// OZ contraction (+ long-range terms in MODE_F), inverse transform, TMA out.
+// tm: W as {2 Nhp, N1, m N2} scalars, box {2B, 1, N2}.
+template <typename T, int MODE, int N, int B, int MS>
+__global__ void __launch_bounds__(Split<N>::R1 * B) k_z_s(Geo g, const __grid_constant__ CUtensorMap tm,
+                                                         const typename Cx<T>::type *__restrict__ twg,
+                                                         ZParams<T> zp, int *__restrict__ err) {
+  using V = typename Cx<T>::type;
+  constexpr int NTHR = Split<N>::R1 * B;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int m = g.m;
+  V *buf = reinterpret_cast<V *>(smem_raw);
+  V *tw = buf + m * N * B;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(tw + N);
+  const int tid = threadIdx.x;
+  const int kx0 = blockIdx.x * B, y = blockIdx.y;
+  if (tid == 0) mbar_init(bar, 1);
+  __syncthreads();
+  if (tid == 0) {
+    mbar_expect_tx(bar, (uint32_t)(m * N * B * sizeof(V)));
+    for (int s = 0; s < m; ++s) tma_load_3d(buf + s * N * B, &tm, bar, 2 * kx0, y, s * g.N2);
+  }
+  for (int q = tid; q < N; q += NTHR) tw[q] = twg[q];
+  if (!mbar_wait(bar, 0, kMbarPolls)) {
+    if (tid == 0) atomicExch(err, 2);
+    return;
+  }
+  __syncthreads();
+  z_tile<T, MODE, N, B, MS>(g, buf, tw, zp, kx0, y);
   fence_proxy_async();
   __syncthreads();
   if (tid == 0) {
@@ -337,6 +350,68 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_z_s(Geo g, const __grid_co
     tma_commit();
     tma_wait_read0();
   }
+}
+
+// The z pass from persistent CTAs with two tile buffers: the TMA load of the
+// next tile is in flight while the current one is transformed, and the
+// store of a tile drains while the next is transformed.  Tiles t =
+// blockIdx.x, blockIdx.x + gridDim.x, ... (kx-block t % nkx, ky t / nkx).
+template <typename T, int MODE, int N, int B, int MS>
+__global__ void __launch_bounds__(Split<N>::R1 * B) k_z_sp(Geo g, const __grid_constant__ CUtensorMap tm,
+                                                          const typename Cx<T>::type *__restrict__ twg,
+                                                          ZParams<T> zp, int *__restrict__ err) {
+  using V = typename Cx<T>::type;
+  constexpr int NTHR = Split<N>::R1 * B;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int m = g.m;
+  V *bufs[2];
+  bufs[0] = reinterpret_cast<V *>(smem_raw);
+  bufs[1] = bufs[0] + m * N * B;
+  V *tw = bufs[1] + m * N * B;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(tw + N);
+  const int tid = threadIdx.x;
+  const int nkx = (g.Nh + B - 1) / B;
+  const int ntile = nkx * g.N1;
+  const uint32_t bytes = (uint32_t)(m * N * B * sizeof(V));
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+  }
+  __syncthreads();
+  int t = blockIdx.x;
+  if (tid == 0 && t < ntile) {
+    mbar_expect_tx(&bar[0], bytes);
+    for (int s = 0; s < m; ++s) tma_load_3d(bufs[0] + s * N * B, &tm, &bar[0], 2 * (t % nkx) * B, t / nkx, s * g.N2);
+  }
+  for (int q = tid; q < N; q += NTHR) tw[q] = twg[q];
+  for (int it = 0; t < ntile; t += gridDim.x, ++it) {
+    const int cur = it & 1;
+    const int tn = t + gridDim.x;
+    if (tid == 0 && tn < ntile) {
+      // the other buffer's last store must have read shared memory first
+      tma_wait_read0();
+      mbar_expect_tx(&bar[cur ^ 1], bytes);
+      for (int s = 0; s < m; ++s)
+        tma_load_3d(bufs[cur ^ 1] + s * N * B, &tm, &bar[cur ^ 1], 2 * (tn % nkx) * B, tn / nkx, s * g.N2);
+    }
+    if (!mbar_wait(&bar[cur], (uint32_t)((it >> 1) & 1), kMbarPolls)) {
+      if (tid == 0) {
+        atomicExch(err, 2);
+        tma_wait0();
+      }
+      return;
+    }
+    __syncthreads();
+    const int kx0 = (t % nkx) * B, y = t / nkx;
+    z_tile<T, MODE, N, B, MS>(g, bufs[cur], tw, zp, kx0, y);
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      for (int s = 0; s < m; ++s) tma_store_3d(&tm, bufs[cur] + s * N * B, 2 * kx0, y, s * g.N2);
+      tma_commit();
+    }
+  }
+  if (tid == 0) tma_wait0();
 }
 
 }  // namespace rism

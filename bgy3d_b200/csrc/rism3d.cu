@@ -255,6 +255,7 @@ struct rism3d_ctx {
   // with TMA descriptors of W for the y and z tiles
   bool stat[2] = {false, false};
   int zb[2] = {4, 8};  // z tile width of the shape-specialised z pass ([0] FP64, [1] FP32: 8 or 4)
+  bool zpers[2] = {false, false};  // that z pass from persistent double-buffered CTAs
   CUtensorMap tmy[2], tmz[2];
   int *d_err = nullptr;  // set by a kernel whose bounded wait timed out
 
@@ -371,6 +372,9 @@ template <typename T, int N> constexpr size_t ys_smem() {
 template <typename T, int N> size_t zs_smem(int m, int B = static_Bz<T>()) {
   return sizeof(typename Cx<T>::type) * (size_t)(m * N * B + N) + 16;
 }
+template <typename T, int N> size_t zsp_smem(int m) {  // two tile buffers, two mbarriers
+  return sizeof(typename Cx<T>::type) * (size_t)(2 * m * N * static_Bz<T>() + N) + 16;
+}
 // Lengths with shape-specialised passes: the coarse grids (48, 96) and the
 // even 2^a 3^b grids of the many-solute workloads whose two-step split fits
 // the register transforms (108 and 162 do not: no split of 54 / odd 81).
@@ -444,6 +448,7 @@ template <typename T, bool INV> void launch_y(rism3d_ctx *c) {
 }
 
 void allow_smem(const void *fn, size_t need);
+unsigned persistent_grid(const void *fn, size_t smem, unsigned work, int threads);
 
 // z pass of a pure-solvent context (solvent.cuh), FP64, for MS solvent sites.
 template <int MODE, int MS> void launch_oz_ms(rism3d_ctx *c) {
@@ -505,7 +510,13 @@ template <typename T, int MODE> void launch_z(rism3d_ctx *c) {
     switch (c->g.N2) {
 #define Z_CASE(N)                                                                                          \
   case N:                                                                                                  \
-    if (B == BW)                                                                                           \
+    if (B == BW && c->zpers[sizeof(T) == 8 ? 0 : 1]) {                                                     \
+      const unsigned nt = (unsigned)(((c->g.Nh + BW - 1) / BW) * c->g.N1);                                 \
+      const size_t sm = zsp_smem<T, N>(c->m);                                                               \
+      const void *fn = (const void *)k_z_sp<T, MODE, N, BW, 3>;                                             \
+      k_z_sp<T, MODE, N, BW, 3><<<persistent_grid(fn, sm, nt, Split<N>::R1 * BW), Split<N>::R1 * BW, sm,    \
+                                  c->stream>>>(c->g, tm, tw, zp, c->d_err);                                \
+    } else if (B == BW)                                                                                    \
       k_z_s<T, MODE, N, BW, 3><<<grid, Split<N>::R1 * BW, zs_smem<T, N>(c->m, BW), c->stream>>>(c->g, tm, tw, \
                                                                                                zp, c->d_err); \
     else                                                                                                   \
@@ -854,13 +865,13 @@ void transfer_axis(rism3d_ctx *c, int outer, int n_in, int n_out, int inner, con
   CKL();
 }
 
-// CTAs of a persistent kernel: as many as fit on the device at once (256
-// threads, `smem` dynamic bytes), at most `work` (the batches to walk).
-unsigned persistent_grid(const void *fn, size_t smem, unsigned work) {
+// CTAs of a persistent kernel: as many as fit on the device at once
+// (`threads` per CTA, `smem` dynamic bytes), at most `work` (the items to walk).
+unsigned persistent_grid(const void *fn, size_t smem, unsigned work, int threads) {
   int dev = 0, sms = 0, per = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 256, smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, smem));
   const unsigned n = (unsigned)std::max(1, per) * (unsigned)std::max(1, sms);
   return std::max(1u, std::min(n, work));
 }
@@ -882,7 +893,7 @@ template <typename T> bool fx_restrict(rism3d_ctx *c, long long rows, const T *i
   case M: {                                                                                                    \
     const size_t sm = fx_smem_restrict<M, kFxRX>(K, c->Nc[0]);                                                           \
     if (sm > 48 * 1024) return false;                                                                         \
-    k_restrict_fx<T, M, kFxRX><<<persistent_grid((const void *)k_restrict_fx<T, M, kFxRX>, sm, nb), 256, sm,     \
+    k_restrict_fx<T, M, kFxRX><<<persistent_grid((const void *)k_restrict_fx<T, M, kFxRX>, sm, nb, 256), 256, sm,     \
                                  c->stream>>>(rows, c->Nc[0], K, in, (float)s, post, tw, c->tC, c->tA);           \
     break;                                                                                                     \
   }
@@ -904,7 +915,7 @@ template <typename T> bool fx_prolong(rism3d_ctx *c, long long rows, const T *r,
   case M: {                                                                                                    \
     const size_t sm = fx_smem_prolong<M, kFxRX>(K, c->Nc[0]);                                                  \
     if (sm > 48 * 1024) return false;                                                                         \
-    k_prolong_fx<T, T, M, kFxRX><<<persistent_grid((const void *)k_prolong_fx<T, T, M, kFxRX>, sm, nb), 256, sm,  \
+    k_prolong_fx<T, T, M, kFxRX><<<persistent_grid((const void *)k_prolong_fx<T, T, M, kFxRX>, sm, nb, 256), 256, sm,  \
                                    c->stream>>>(rows, c->Nc[0], K, c->tA, post, tw, c->tD, r, s, out);            \
     break;                                                                                                     \
   }
@@ -1674,6 +1685,7 @@ struct TuneVal {
   TileShape t[2];
   bool stat[2];
   int zb[2];
+  bool zpers[2];
 };
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int, int>, TuneVal> g_tune;
@@ -1758,13 +1770,35 @@ template <typename T> void tune_precision(rism3d_ctx *c, const T *A, const T *Bv
     } else {
       c->zb[pr] = wide;
       make_tmap(c, &c->tmz[pr], pr == 0, wide, 1, G.N2);
+      // persistent double-buffered CTAs for the wide tiles
+      c->zpers[pr] = true;
+      const float p_ms = time_ms(c, run, reps);
+      if (p_ms < 0.97f * s_ms) s_ms = p_ms;
+      else c->zpers[pr] = false;
     }
     c->stat[pr] = s_ms <= 1.05f * g_ms;  // keep the specialised passes unless clearly slower
   }
 }
 
+// RISM3D_Z_PERSISTENT=1 / 0 forces the persistent z pass on / off where the
+// shape-specialised passes run (the tests compare both).
+void force_z_persistent(rism3d_ctx *c) {
+  const char *env = std::getenv("RISM3D_Z_PERSISTENT");
+  if (!env || (env[0] != '0' && env[0] != '1')) return;
+  const int wide[2] = {static_Bz<double>(), static_Bz<float>()};
+  for (int pr = 0; pr < 2; ++pr) {
+    if (!c->stat[pr]) continue;
+    if (c->zb[pr] != wide[pr]) {
+      c->zb[pr] = wide[pr];
+      make_tmap(c, &c->tmz[pr], pr == 0, wide[pr], 1, c->g.N2);
+    }
+    c->zpers[pr] = env[0] == '1';
+  }
+}
+
 // Applies the cached shapes of this context's (grid, fields) or times them.
 void autotune(rism3d_ctx *c) {
+  struct Force { rism3d_ctx *c; ~Force() { force_z_persistent(c); } } force{c};
   const char *env = std::getenv("RISM3D_AUTOTUNE");
   if (env && env[0] == '0') return;
   const Geo &G = c->g;
@@ -1777,6 +1811,7 @@ void autotune(rism3d_ctx *c) {
       for (int pr = 0; pr < 2; ++pr) {
         c->tiles[pr] = it->second.t[pr];
         c->stat[pr] = c->stat[pr] && it->second.stat[pr];
+        c->zpers[pr] = c->stat[pr] && it->second.zpers[pr];
         if (c->stat[pr] && c->zb[pr] != it->second.zb[pr]) {
           c->zb[pr] = it->second.zb[pr];
           make_tmap(c, &c->tmz[pr], pr == 0, c->zb[pr], 1, G.N2);
@@ -1805,6 +1840,7 @@ void autotune(rism3d_ctx *c) {
     v.t[pr] = c->tiles[pr];
     v.stat[pr] = c->stat[pr];
     v.zb[pr] = c->zb[pr];
+    v.zpers[pr] = c->zpers[pr];
   }
   g_tune[key] = v;
 }
@@ -2083,7 +2119,8 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
     OPTIN_Z(float)
 #undef OPTIN_Z
     if (c->stat[0]) {
-      need = std::max({xs_smem<double, 128>(), ys_smem<double, 256>(), zs_smem<double, 256>(m),
+      need = std::max({xs_smem<double, 128>(), ys_smem<double, 256>(), zsp_smem<double, 256>(m),
+                       zsp_smem<float, 256>(m), zs_smem<double, 256>(m),
                        xs_smem<float, 128>(), ys_smem<float, 256>(), zs_smem<float, 256>(m)});
 #define OPTIN_S(T)                                               \
   allow((const void *)k_xfwd_s<T, MODE_F, 24, kStaticRX>);       \
@@ -2157,7 +2194,23 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
   allow((const void *)k_z_s<T, MODE_F, 192, static_Bz<T>() / 2, 3>); \
   allow((const void *)k_z_s<T, MODE_J, 192, static_Bz<T>() / 2, 3>); \
   allow((const void *)k_z_s<T, MODE_F, 256, static_Bz<T>() / 2, 3>); \
-  allow((const void *)k_z_s<T, MODE_J, 256, static_Bz<T>() / 2, 3>);
+  allow((const void *)k_z_s<T, MODE_J, 256, static_Bz<T>() / 2, 3>); \
+  allow((const void *)k_z_sp<T, MODE_F, 48, static_Bz<T>(), 3>);    \
+  allow((const void *)k_z_sp<T, MODE_J, 48, static_Bz<T>(), 3>);    \
+  allow((const void *)k_z_sp<T, MODE_F, 64, static_Bz<T>(), 3>);    \
+  allow((const void *)k_z_sp<T, MODE_J, 64, static_Bz<T>(), 3>);    \
+  allow((const void *)k_z_sp<T, MODE_F, 72, static_Bz<T>(), 3>);    \
+  allow((const void *)k_z_sp<T, MODE_J, 72, static_Bz<T>(), 3>);    \
+  allow((const void *)k_z_sp<T, MODE_F, 96, static_Bz<T>(), 3>);    \
+  allow((const void *)k_z_sp<T, MODE_J, 96, static_Bz<T>(), 3>);    \
+  allow((const void *)k_z_sp<T, MODE_F, 128, static_Bz<T>(), 3>);   \
+  allow((const void *)k_z_sp<T, MODE_J, 128, static_Bz<T>(), 3>);   \
+  allow((const void *)k_z_sp<T, MODE_F, 144, static_Bz<T>(), 3>);   \
+  allow((const void *)k_z_sp<T, MODE_J, 144, static_Bz<T>(), 3>);   \
+  allow((const void *)k_z_sp<T, MODE_F, 192, static_Bz<T>(), 3>);   \
+  allow((const void *)k_z_sp<T, MODE_J, 192, static_Bz<T>(), 3>);   \
+  allow((const void *)k_z_sp<T, MODE_F, 256, static_Bz<T>(), 3>);   \
+  allow((const void *)k_z_sp<T, MODE_J, 256, static_Bz<T>(), 3>);
       OPTIN_S(double)
       OPTIN_S(float)
 #undef OPTIN_S
@@ -2768,7 +2821,7 @@ int rism3d_tile_shapes(rism3d_ctx *ctx, int *out) {
     out[3 * pr + 1] = ctx->tiles[pr].BY;
     out[3 * pr + 2] = ctx->tiles[pr].BZ;
     out[6 + pr] = ctx->stat[pr] ? 1 : 0;
-    out[8 + pr] = ctx->zb[pr];
+    out[8 + pr] = ctx->zb[pr] * (ctx->zpers[pr] ? -1 : 1);  // negative: persistent CTAs
   }
   return RISM3D_OK;
 }

@@ -293,7 +293,8 @@ int rism3d_response(rism3d_ctx *ctx, const double *T, rism3d_grad *grad);
    columns per CTA of the runtime-length passes for FP64 (out[0..2]) and
    FP32 (out[3..5]), whether the shape-specialised passes run (out[6]
    FP64, out[7] FP32) and the z-column width of their z pass (out[8],
-   out[9]).  Chosen when the context is created by timing the
+   out[9]; negative when that pass runs from persistent double-buffered
+   CTAs).  Chosen when the context is created by timing the
    candidates on its own buffers, once per grid shape and process
    (RISM3D_AUTOTUNE=0: a register / occupancy rule instead). */
 int rism3d_tile_shapes(rism3d_ctx *ctx, int *out);

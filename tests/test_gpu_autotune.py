@@ -60,3 +60,25 @@ def test_tuned_schedule_matches_rule(fixture_loader, N):
                 assert np.max(np.abs(x - y)) <= tol * max(1.0, np.max(np.abs(y)))
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("N", [48, 96, 256])
+def test_persistent_z_pass_is_bitwise(fixture_loader, N, monkeypatch):
+    """The persistent double-buffered z pass computes the same tiles as the
+    one-tile-per-CTA pass: identical F and J.v, FP64 and FP32."""
+    meta, arr = fixture_loader("synth6_kh_n32")
+    s = settings_of(meta, N=N, L=12.0 if N <= 128 else 36.0, **{"coarse-h": 0})  # |k| inside the chi table
+    monkeypatch.setenv("RISM3D_Z_PERSISTENT", "1")
+    a = RismContext(meta["solute"], meta["solvent"], s, arr["chi"])
+    monkeypatch.setenv("RISM3D_Z_PERSISTENT", "0")
+    b = RismContext(meta["solute"], meta["solvent"], s, arr["chi"])
+    ta, tb = a.tile_shapes(), b.tile_shapes()
+    assert ta["f32"][4] < 0 and ta["f64"][4] < 0 and tb["f32"][4] > 0
+    g = torch.Generator(device="cuda").manual_seed(3)
+    for dt in (torch.float64, torch.float32):
+        T = (torch.randn(a.shape, generator=g, device="cuda", dtype=torch.float64) * 0.1).to(dt)
+        dT = (torch.randn(a.shape, generator=g, device="cuda", dtype=torch.float64) * 0.1).to(dt)
+        assert torch.equal(a.iterate_t1(T)[0], b.iterate_t1(T)[0])
+        assert torch.equal(a.jacobian_t1(T, dT), b.jacobian_t1(T, dT))
+    a.close()
+    b.close()
