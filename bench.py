@@ -62,9 +62,11 @@ SETTINGS = {"L": 24.0, "rho": 0.0333295, "beta": 1.6889, "closure": "KH", "rmax"
 # scale the CPU samples.
 FP64_SOLVE_EVALS = {"f": 9, "jv": 464}
 PLAIN_FP64 = {"precision": "fp64", "coarse-h": 0, "ew-forcing": 0, "krylov-restart": 30}
-# DRAM bytes (read + write) of one FP32 z-pass launch at 256^3, measured by
-# ncu --set full on the shape-specialised kernel (273 MB read, 155 MB write).
-ZPASS_TRAFFIC = 427.6e6
+# DRAM bytes (read + write) of the five FP32 passes of one Jacobian product at
+# 256^3 (x-forward 576.0, y 352.9, z 351.7, y-inverse 352.8, x-inverse
+# 574.1 MB), measured by ncu dram__bytes_read.sum + dram__bytes_write.sum on
+# the shape-specialised kernels.
+JV_TRAFFIC = 2207.5e6
 
 
 def workload(grid=GRID):
@@ -479,13 +481,16 @@ def run_ours(args, rank, world):
 
     m = 3
     bw, src = hbm_peak()
-    # roofline of the FP32 z pass (the costliest FFT pass of the mixed solve
-    # and the kernel of the ncu capture whose DRAM traffic is quoted)
-    k, prec = "z", "f32"
-    lau = {kk: prof[(kk, prec)][1] for kk in ("xfwd", "y", "z", "xinv")}
-    byt = pass_bytes(args.grid, m, 4, lau, res["f-evals-fp32"])[k]
-    t_ms, n = prof[(k, prec)]
-    achieved = byt / n / (t_ms / n * 1e-3) / 1e9
+    # roofline of the FFT passes of F and J.v (FP32): the five fused passes
+    # that evaluate the path's residual and Jacobian products
+    prec = "f32"
+    passes = ("xfwd", "y", "z", "xinv")
+    lau = {kk: prof[(kk, prec)][1] for kk in passes}
+    byt_all = pass_bytes(args.grid, m, 4, lau, res["f-evals-fp32"])
+    pms = {kk: prof[(kk, prec)][0] for kk in passes}
+    achieved = sum(byt_all.values()) / (sum(pms.values()) * 1e-3) / 1e9
+    evals = res["f-evals-fp32"] + res["jv-evals-fp32"]
+    pass_gbs = {kk: byt_all[kk] / (pms[kk] * 1e-3) / 1e9 for kk in passes if pms[kk] > 0}
     total_ms = sum(v[0] for v in prof.values())
     value = world * args.steps / (ms * 1e-3)
     line = {
@@ -511,11 +516,13 @@ def run_ours(args, rank, world):
                   "f_evals_f64": res["f-evals"], "jv_evals_f64": res["jv-evals"],
                   "f_evals_f32": res["f-evals-fp32"], "jv_evals_f32": res["jv-evals-fp32"],
                   "jv_evals_coarse": res["jv-evals-coarse"]},
-        "roofline": {"bound": "hbm", "kernel": f"{k} pass ({prec})", "achieved": achieved, "peak": bw,
-                     "peak_source": src, "unit": "GB/s", "frac": achieved / bw, "traffic": ZPASS_TRAFFIC,
-                     "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one FP32 z-pass "
-                                     "launch at 256^3 (F mode: W read + write, L read)",
-                     "bytes_per_launch": byt / n, "share_of_solve": t_ms / total_ms,
+        "roofline": {"bound": "hbm", "kernel": "F / J.v FFT passes (FP32: x-forward, y, z, y-inverse, x-inverse)",
+                     "achieved": achieved, "peak": bw, "peak_source": src, "unit": "GB/s", "frac": achieved / bw,
+                     "traffic": JV_TRAFFIC,
+                     "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the five FP32 passes "
+                                     "of one J.v at 256^3 (per launch of the pipeline)",
+                     "bytes_per_launch": sum(byt_all.values()) / max(evals, 1),
+                     "share_of_solve": sum(pms.values()) / total_ms, "pass_gbs": pass_gbs,
                      "passes_ms": {f"{a}/{p}": round(v[0], 3) for (a, p), v in prof.items() if v[1]}},
         "e2e": {"value": 1.0 / e2e_s, "unit": "solves/s",
                 "h2d_bytes_per_step": int(chi.nbytes + 2 * 64 * (N_SITES + 3)),
