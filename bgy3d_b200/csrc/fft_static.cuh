@@ -72,9 +72,10 @@ template <bool INV, typename V> struct RDft<4, INV, V> {
 };
 
 // First-step radix of a compile-time length: the largest of 16, 8, 12, 6, 4
-// dividing N with a cofactor no larger than it.
+// dividing N with a cofactor no larger than it (16 for 512).
 template <int N> struct Split {
-  static constexpr int R1 = (N % 16 == 0 && N / 16 <= 16) ? 16
+  static constexpr int R1 = N == 512 ? 16  // 16 x 32: the second step holds 32 points per thread
+                          : (N % 16 == 0 && N / 16 <= 16) ? 16
                           : (N % 8 == 0 && N / 8 <= 8) ? 8
                           : (N % 12 == 0 && N / 12 <= 12) ? 12
                           : (N % 6 == 0 && N / 6 <= 8) ? 6 : 4;

@@ -189,6 +189,10 @@ __global__ void __launch_bounds__(256) k_xinv_s(Geo g, const typename Cx<T>::typ
   block_norms(amax, sum2, part + (blockIdx.y * gridDim.x + blockIdx.x));
 }
 
+// A TMA box spans at most 256 elements per dimension: tiles along a 512-point
+// axis move as two boxes of kTmaRows rows.
+constexpr int kTmaRows = 256;
+
 // y pass: one [N][B] tile (kx0 .. kx0+B-1 at fixed z, site) by TMA.
 // tm: W as {2 Nhp, N1, m N2} scalars, box {2B, N1, 1}.
 template <typename T, bool INV, int N, int B>
@@ -207,7 +211,8 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_y_s(Geo g, const __grid_co
   __syncthreads();
   if (tid == 0) {
     mbar_expect_tx(bar, (uint32_t)(N * B * sizeof(V)));
-    tma_load_3d(buf, &tm, bar, 2 * kx0, 0, site * g.N2 + z);
+#pragma unroll
+    for (int c = 0; c < N; c += kTmaRows) tma_load_3d(buf + c * B, &tm, bar, 2 * kx0, c, site * g.N2 + z);
   }
   for (int q = tid; q < N; q += NTHR) tw[q] = twg[q];
   if (!mbar_wait(bar, 0, kMbarPolls)) {
@@ -219,7 +224,8 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_y_s(Geo g, const __grid_co
   fence_proxy_async();
   __syncthreads();
   if (tid == 0) {
-    tma_store_3d(&tm, buf, 2 * kx0, 0, site * g.N2 + z);
+#pragma unroll
+    for (int c = 0; c < N; c += kTmaRows) tma_store_3d(&tm, buf + c * B, 2 * kx0, c, site * g.N2 + z);
     tma_commit();
     tma_wait_read0();
   }
@@ -334,7 +340,9 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_z_s(Geo g, const __grid_co
   __syncthreads();
   if (tid == 0) {
     mbar_expect_tx(bar, (uint32_t)(m * N * B * sizeof(V)));
-    for (int s = 0; s < m; ++s) tma_load_3d(buf + s * N * B, &tm, bar, 2 * kx0, y, s * g.N2);
+    for (int s = 0; s < m; ++s)
+#pragma unroll
+      for (int c = 0; c < N; c += kTmaRows) tma_load_3d(buf + s * N * B + c * B, &tm, bar, 2 * kx0, y, s * g.N2 + c);
   }
   for (int q = tid; q < N; q += NTHR) tw[q] = twg[q];
   if (!mbar_wait(bar, 0, kMbarPolls)) {
@@ -346,7 +354,9 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_z_s(Geo g, const __grid_co
   fence_proxy_async();
   __syncthreads();
   if (tid == 0) {
-    for (int s = 0; s < m; ++s) tma_store_3d(&tm, buf + s * N * B, 2 * kx0, y, s * g.N2);
+    for (int s = 0; s < m; ++s)
+#pragma unroll
+      for (int c = 0; c < N; c += kTmaRows) tma_store_3d(&tm, buf + s * N * B + c * B, 2 * kx0, y, s * g.N2 + c);
     tma_commit();
     tma_wait_read0();
   }
@@ -381,7 +391,10 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_z_sp(Geo g, const __grid_c
   int t = blockIdx.x;
   if (tid == 0 && t < ntile) {
     mbar_expect_tx(&bar[0], bytes);
-    for (int s = 0; s < m; ++s) tma_load_3d(bufs[0] + s * N * B, &tm, &bar[0], 2 * (t % nkx) * B, t / nkx, s * g.N2);
+    for (int s = 0; s < m; ++s)
+#pragma unroll
+      for (int c = 0; c < N; c += kTmaRows)
+        tma_load_3d(bufs[0] + s * N * B + c * B, &tm, &bar[0], 2 * (t % nkx) * B, t / nkx, s * g.N2 + c);
   }
   for (int q = tid; q < N; q += NTHR) tw[q] = twg[q];
   for (int it = 0; t < ntile; t += gridDim.x, ++it) {
@@ -392,7 +405,10 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_z_sp(Geo g, const __grid_c
       tma_wait_read0();
       mbar_expect_tx(&bar[cur ^ 1], bytes);
       for (int s = 0; s < m; ++s)
-        tma_load_3d(bufs[cur ^ 1] + s * N * B, &tm, &bar[cur ^ 1], 2 * (tn % nkx) * B, tn / nkx, s * g.N2);
+#pragma unroll
+        for (int c = 0; c < N; c += kTmaRows)
+          tma_load_3d(bufs[cur ^ 1] + s * N * B + c * B, &tm, &bar[cur ^ 1], 2 * (tn % nkx) * B, tn / nkx,
+                      s * g.N2 + c);
     }
     if (!mbar_wait(&bar[cur], (uint32_t)((it >> 1) & 1), kMbarPolls)) {
       if (tid == 0) {
@@ -407,7 +423,10 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_z_sp(Geo g, const __grid_c
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
-      for (int s = 0; s < m; ++s) tma_store_3d(&tm, bufs[cur] + s * N * B, 2 * kx0, y, s * g.N2);
+      for (int s = 0; s < m; ++s)
+#pragma unroll
+        for (int c = 0; c < N; c += kTmaRows)
+          tma_store_3d(&tm, bufs[cur] + s * N * B + c * B, 2 * kx0, y, s * g.N2 + c);
       tma_commit();
     }
   }

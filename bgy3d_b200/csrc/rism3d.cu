@@ -379,10 +379,10 @@ template <typename T, int N> size_t zsp_smem(int m) {  // two tile buffers, two 
 // even 2^a 3^b grids of the many-solute workloads whose two-step split fits
 // the register transforms (108 and 162 do not: no split of 54 / odd 81).
 bool static_len_x(int M) {
-  return M == 24 || M == 32 || M == 36 || M == 48 || M == 64 || M == 72 || M == 96 || M == 128;
+  return M == 24 || M == 32 || M == 36 || M == 48 || M == 64 || M == 72 || M == 96 || M == 128 || M == 256;
 }
 bool static_len_yz(int N) {
-  return N == 48 || N == 64 || N == 72 || N == 96 || N == 128 || N == 144 || N == 192 || N == 256;
+  return N == 48 || N == 64 || N == 72 || N == 96 || N == 128 || N == 144 || N == 192 || N == 256 || N == 512;
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -408,7 +408,9 @@ void make_tmap(rism3d_ctx *c, CUtensorMap *tm, bool fp64, int B, int by, int bz)
   const size_t es = fp64 ? 8 : 4;
   cuuint64_t dims[3] = {(cuuint64_t)(2 * G.Nhp), (cuuint64_t)G.N1, (cuuint64_t)G.N2 * G.m};
   cuuint64_t strides[2] = {(cuuint64_t)(2 * G.Nhp) * es, (cuuint64_t)(2 * G.Nhp) * G.N1 * es};
-  cuuint32_t box[3] = {(cuuint32_t)(2 * B), (cuuint32_t)by, (cuuint32_t)bz};
+  // a box spans at most 256 elements per dimension (the kernels move
+  // 512-point tiles as two boxes)
+  cuuint32_t box[3] = {(cuuint32_t)(2 * B), (cuuint32_t)std::min(by, 256), (cuuint32_t)std::min(bz, 256)};
   cuuint32_t estr[3] = {1, 1, 1};
   const CUresult r = encode_fn()(tm, fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
                                  c->W, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -433,7 +435,7 @@ template <typename T, bool INV> void launch_y(rism3d_ctx *c) {
   case N:                                                                                           \
     k_y_s<T, INV, N, B><<<grid, Split<N>::R1 * B, ys_smem<T, N>(), c->stream>>>(c->g, tm, tw, c->d_err); \
     break;
-      Y_CASE(48) Y_CASE(64) Y_CASE(72) Y_CASE(96) Y_CASE(128) Y_CASE(144) Y_CASE(192) Y_CASE(256)
+      Y_CASE(48) Y_CASE(64) Y_CASE(72) Y_CASE(96) Y_CASE(128) Y_CASE(144) Y_CASE(192) Y_CASE(256) Y_CASE(512)
 #undef Y_CASE
     }
     CKL();
@@ -523,7 +525,7 @@ template <typename T, int MODE> void launch_z(rism3d_ctx *c) {
       k_z_s<T, MODE, N, BN, 3><<<grid, Split<N>::R1 * BN, zs_smem<T, N>(c->m, BN), c->stream>>>(c->g, tm, tw, \
                                                                                                zp, c->d_err); \
     break;
-      Z_CASE(48) Z_CASE(64) Z_CASE(72) Z_CASE(96) Z_CASE(128) Z_CASE(144) Z_CASE(192) Z_CASE(256)
+      Z_CASE(48) Z_CASE(64) Z_CASE(72) Z_CASE(96) Z_CASE(128) Z_CASE(144) Z_CASE(192) Z_CASE(256) Z_CASE(512)
 #undef Z_CASE
     }
     CKL();
@@ -579,6 +581,7 @@ int pipeline(rism3d_ctx *c, const T *A, const T *Bv, T p, T sub, T *out) {
                                                                              W, postw<T>(c), twx);      \
     break;
         XF_CASE(24) XF_CASE(32) XF_CASE(36) XF_CASE(48) XF_CASE(64) XF_CASE(72) XF_CASE(96) XF_CASE(128)
+        XF_CASE(256)
 #undef XF_CASE
       }
     } else {
@@ -601,6 +604,7 @@ int pipeline(rism3d_ctx *c, const T *A, const T *Bv, T p, T sub, T *out) {
                                                                        twx, c->npart);                        \
     break;
         XI_CASE(24) XI_CASE(32) XI_CASE(36) XI_CASE(48) XI_CASE(64) XI_CASE(72) XI_CASE(96) XI_CASE(128)
+        XI_CASE(256)
 #undef XI_CASE
       }
     } else {
@@ -2119,9 +2123,9 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
     OPTIN_Z(float)
 #undef OPTIN_Z
     if (c->stat[0]) {
-      need = std::max({xs_smem<double, 128>(), ys_smem<double, 256>(), zsp_smem<double, 256>(m),
-                       zsp_smem<float, 256>(m), zs_smem<double, 256>(m),
-                       xs_smem<float, 128>(), ys_smem<float, 256>(), zs_smem<float, 256>(m)});
+      need = std::max({xs_smem<double, 256>(), ys_smem<double, 512>(), zsp_smem<double, 512>(m),
+                       zsp_smem<float, 512>(m), zs_smem<double, 512>(m),
+                       xs_smem<float, 256>(), ys_smem<float, 512>(), zs_smem<float, 512>(m)});
 #define OPTIN_S(T)                                               \
   allow((const void *)k_xfwd_s<T, MODE_F, 24, kStaticRX>);       \
   allow((const void *)k_xfwd_s<T, MODE_J, 24, kStaticRX>);       \
@@ -2147,6 +2151,17 @@ int create_impl(const rism3d_problem *pd, int m, const rism3d_site *solvent, int
   allow((const void *)k_xfwd_s<T, MODE_F, 128, kStaticRX>);      \
   allow((const void *)k_xfwd_s<T, MODE_J, 128, kStaticRX>);      \
   allow((const void *)k_xinv_s<T, 128, kStaticRX>);              \
+  allow((const void *)k_xfwd_s<T, MODE_F, 256, kStaticRX>);      \
+  allow((const void *)k_xfwd_s<T, MODE_J, 256, kStaticRX>);      \
+  allow((const void *)k_xinv_s<T, 256, kStaticRX>);              \
+  allow((const void *)k_y_s<T, false, 512, static_B<T>()>);      \
+  allow((const void *)k_y_s<T, true, 512, static_B<T>()>);       \
+  allow((const void *)k_z_s<T, MODE_F, 512, static_Bz<T>(), 3>); \
+  allow((const void *)k_z_s<T, MODE_J, 512, static_Bz<T>(), 3>); \
+  allow((const void *)k_z_s<T, MODE_F, 512, static_Bz<T>() / 2, 3>); \
+  allow((const void *)k_z_s<T, MODE_J, 512, static_Bz<T>() / 2, 3>); \
+  allow((const void *)k_z_sp<T, MODE_F, 512, static_Bz<T>(), 3>);   \
+  allow((const void *)k_z_sp<T, MODE_J, 512, static_Bz<T>(), 3>);   \
   allow((const void *)k_y_s<T, false, 48, static_B<T>()>);       \
   allow((const void *)k_y_s<T, true, 48, static_B<T>()>);        \
   allow((const void *)k_z_s<T, MODE_F, 48, static_Bz<T>(), 3>);  \
