@@ -451,6 +451,7 @@ template <typename T, bool INV> void launch_y(rism3d_ctx *c) {
 
 void allow_smem(const void *fn, size_t need);
 unsigned persistent_grid(const void *fn, size_t smem, unsigned work, int threads);
+int optin_limit();
 
 // z pass of a pure-solvent context (solvent.cuh), FP64, for MS solvent sites.
 template <int MODE, int MS> void launch_oz_ms(rism3d_ctx *c) {
@@ -884,6 +885,8 @@ unsigned persistent_grid(const void *fn, size_t smem, unsigned work, int threads
 // shape-specialised transform; false: use the dense tiles.
 constexpr int kFxRX = 16;
 bool fx_usable(const rism3d_ctx *c) {
+  const char *dense = std::getenv("RISM3D_DENSE_TRANSFERS");  // 1: the dense tiles everywhere (tests)
+  if (dense && dense[0] == '1') return false;
   return c->tC && static_len_x(c->g.M) && c->Nc[0] % 2 == 0 && c->Nc[0] / 2 < c->g.M;
 }
 template <typename T> bool fx_restrict(rism3d_ctx *c, long long rows, const T *in, double s) {
@@ -895,13 +898,14 @@ template <typename T> bool fx_restrict(rism3d_ctx *c, long long rows, const T *i
   switch (c->g.M) {
 #define FXR(M)                                                                                                 \
   case M: {                                                                                                    \
-    const size_t sm = fx_smem_restrict<M, kFxRX>(K, c->Nc[0]);                                                           \
-    if (sm > 48 * 1024) return false;                                                                         \
+    const size_t sm = fx_smem_restrict<M, kFxRX>(K, c->Nc[0]);                                                \
+    if ((long long)sm > optin_limit()) return false;                                                          \
+    if (sm > 48 * 1024) allow_smem((const void *)k_restrict_fx<T, M, kFxRX>, sm);                             \
     k_restrict_fx<T, M, kFxRX><<<persistent_grid((const void *)k_restrict_fx<T, M, kFxRX>, sm, nb, 256), 256, sm,     \
                                  c->stream>>>(rows, c->Nc[0], K, in, (float)s, post, tw, c->tC, c->tA);           \
     break;                                                                                                     \
   }
-    FXR(24) FXR(32) FXR(36) FXR(48) FXR(64) FXR(72) FXR(96) FXR(128)
+    FXR(24) FXR(32) FXR(36) FXR(48) FXR(64) FXR(72) FXR(96) FXR(128) FXR(256)
 #undef FXR
     default: return false;
   }
@@ -918,12 +922,13 @@ template <typename T> bool fx_prolong(rism3d_ctx *c, long long rows, const T *r,
 #define FXP(M)                                                                                                 \
   case M: {                                                                                                    \
     const size_t sm = fx_smem_prolong<M, kFxRX>(K, c->Nc[0]);                                                  \
-    if (sm > 48 * 1024) return false;                                                                         \
+    if ((long long)sm > optin_limit()) return false;                                                          \
+    if (sm > 48 * 1024) allow_smem((const void *)k_prolong_fx<T, T, M, kFxRX>, sm);                           \
     k_prolong_fx<T, T, M, kFxRX><<<persistent_grid((const void *)k_prolong_fx<T, T, M, kFxRX>, sm, nb, 256), 256, sm,  \
                                    c->stream>>>(rows, c->Nc[0], K, c->tA, post, tw, c->tD, r, s, out);            \
     break;                                                                                                     \
   }
-    FXP(24) FXP(32) FXP(36) FXP(48) FXP(64) FXP(72) FXP(96) FXP(128)
+    FXP(24) FXP(32) FXP(36) FXP(48) FXP(64) FXP(72) FXP(96) FXP(128) FXP(256)
 #undef FXP
     default: return false;
   }
