@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librism3d.so")
-SOURCES = ["rism3d.cu", "rism1d.cpp", "noalloc.cu"]
+SOURCES = ["rism3d.cu", "twogrid_fx2.cu", "rism1d.cpp", "noalloc.cu"]
 HEADERS = ["fft_core.cuh", "kernels.cuh", "fft_static.cuh", "kernels_static.cuh", "krylov.cuh", "twogrid.cuh",
            "twogrid_fft.cuh", "grad.cuh", "solvent.cuh", "info.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -34,14 +34,22 @@ def build(force=False, verbose_ptxas=False):
         return LIB
     # per-thread default streams: host threads of the batch driver issue
     # independently; each still orders against torch's legacy stream
-    cmd = [NVCC, "-O3", "-std=c++17", "-lineinfo", "--default-stream", "per-thread",
-           "-gencode", "arch=compute_100a,code=sm_100a",
-           "-Xcompiler", "-fPIC,-O3", "-shared",
-           "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-           "-o", LIB + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES]
+    flags = ["-O3", "-std=c++17", "-lineinfo", "--default-stream", "per-thread",
+             "-gencode", "arch=compute_100a,code=sm_100a",
+             "-Xcompiler", "-fPIC,-O3",
+             "-I", os.path.join(ROOT, "include"), "-I", CSRC]
     if verbose_ptxas:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
+        flags.insert(0, "-Xptxas=-v")
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs = [os.path.join(objdir, os.path.splitext(s)[0] + ".o") for s in SOURCES]
+    # one nvcc per source, concurrently (the translation units share no device code)
+    procs = [subprocess.Popen([NVCC] + flags + ["-c", "-o", o, os.path.join(CSRC, s)])
+             for s, o in zip(SOURCES, objs)]
+    codes = [p.wait() for p in procs]
+    if any(codes):
+        raise subprocess.CalledProcessError(max(codes), "nvcc")
+    subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB + ".tmp"] + objs, check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

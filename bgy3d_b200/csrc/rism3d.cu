@@ -37,6 +37,16 @@
 
 using namespace rism;
 
+namespace rism {  // twogrid_fx2.cu: x transfers with both sides by FFT
+bool fx2_has_pair(int M, int MC);
+template <typename T>
+bool fx2_restrict(int M, int MC, long long rows, const T *in, float s, const float2 *post, const float2 *tw,
+                  const float2 *postc, const float2 *twc, float *out, cudaStream_t st);
+template <typename T>
+bool fx2_prolong(int M, int MC, long long rows, const float *y, const float2 *post, const float2 *tw,
+                 const float2 *postc, const float2 *twc, const T *r, double s, T *out, cudaStream_t st);
+}  // namespace rism
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -889,11 +899,24 @@ bool fx_usable(const rism3d_ctx *c) {
   if (dense && dense[0] == '1') return false;
   return c->tC && static_len_x(c->g.M) && c->Nc[0] % 2 == 0 && c->Nc[0] / 2 < c->g.M;
 }
+// Both sides by FFT (twogrid_fx2.cu) where the coarse half row also has a
+// shape-specialised transform; RISM3D_DENSE_TRANSFERS=2 keeps the (K+1) x Nc
+// table product on the coarse side (tests compare the two).
+bool fx2_usable(const rism3d_ctx *c) {
+  const char *dense = std::getenv("RISM3D_DENSE_TRANSFERS");
+  if (dense && dense[0] == '2') return false;
+  return c->coarse && c->coarse->g.M == c->Nc[0] / 2 && rism::fx2_has_pair(c->g.M, c->Nc[0] / 2);
+}
 template <typename T> bool fx_restrict(rism3d_ctx *c, long long rows, const T *in, double s) {
   if (!fx_usable(c)) return false;
   const int K = c->Nc[0] / 2;
   const auto *post = postw<float>(c);
   const auto *tw = static_cast<const float2 *>(c->plan<float>(0).tw);
+  if (fx2_usable(c) && rism::fx2_restrict<T>(c->g.M, c->Nc[0] / 2, rows, in, (float)s, post, tw, c->coarse->post32,
+                                              c->coarse->tw32[0], c->tA, c->stream)) {
+    CKL();
+    return true;
+  }
   const unsigned nb = (unsigned)((rows + kFxRX - 1) / kFxRX);
   switch (c->g.M) {
 #define FXR(M)                                                                                                 \
@@ -917,6 +940,11 @@ template <typename T> bool fx_prolong(rism3d_ctx *c, long long rows, const T *r,
   const int K = c->Nc[0] / 2;
   const auto *post = postw<float>(c);
   const auto *tw = static_cast<const float2 *>(c->plan<float>(0).tw);
+  if (fx2_usable(c) && rism::fx2_prolong<T>(c->g.M, c->Nc[0] / 2, rows, c->tA, post, tw, c->coarse->post32,
+                                             c->coarse->tw32[0], r, s, out, c->stream)) {
+    CKL();
+    return true;
+  }
   const unsigned nb = (unsigned)((rows + kFxRX - 1) / kFxRX);
   switch (c->g.M) {
 #define FXP(M)                                                                                                 \

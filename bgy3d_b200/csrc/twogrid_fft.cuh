@@ -283,3 +283,238 @@ __global__ void __launch_bounds__(256) k_prolong_fx(long long rows, int Nc, int 
 }
 
 }  // namespace rism
+
+namespace rism {
+
+// ---- both sides by FFT: the coarse side as a packed row transform of
+// length Nc = 2 MC instead of the (K+1) x Nc table product (K = MC).
+//
+// Restriction: out = c2r_Nc(X_0..X_K) / N0 (Im X_0, Im X_K dropped, as the
+// table's c_k weights do), i.e. the K+1 kept coefficients are packed into
+// MC complex values and transformed by the MC-point inverse FFT; the packed
+// result z_j = out_{2j} + i out_{2j+1}.
+// Prolongation: X_k = f_k r2c_Nc(y)_k from the MC-point forward FFT of the
+// coarse row and its untangle, then the fine packed c2r as before.
+// twc / postc: the twiddles of the MC-point transform and exp(-2 pi i k / Nc),
+// k in [0, MC] (the coarse grid's own x tables).  The coarse row tile
+// aliases the fine one (it is only live while the fine one is not).
+template <int M, int MC, int RX> __host__ __device__ constexpr int fx2_words() {
+  return M + fx_buf<M, RX>() + RX * (MC + 1) + MC;
+}
+template <int M, int MC, int RX> inline size_t fx2_smem() { return sizeof(float2) * (size_t)fx2_words<M, MC, RX>(); }
+
+// z-pack of a Hermitian half spectrum X_0..X_K (row stride K1) for the packed
+// c2r of length 2 MM (K >= MM: only X_0..X_MM are read; K < MM: zero above
+// K).  Writes the MM packed values of every row into buf (layout L).
+template <int MM, int RX, class L>
+__device__ __forceinline__ void fx_pack_c2r(const float2 *X, int K, int K1, const float2 *post, float2 *buf) {
+  constexpr int H = MM / 2 + 1;
+  for (int e = threadIdx.x; e < RX * H; e += 256) {
+    const int row = e / H, k = e - row * H;
+    float2 xk = make_float2(0.f, 0.f), xm = make_float2(0.f, 0.f);
+    if (k <= K) xk = X[row * K1 + k];
+    if (MM - k <= K) xm = X[row * K1 + (MM - k)];
+    if (k == 0) { xk.y = 0.f; xm.y = 0.f; }
+    float2 Aa, Dd;
+    Aa.x = xk.x + xm.x; Aa.y = xk.y - xm.y;
+    Dd.x = xk.x - xm.x; Dd.y = xk.y + xm.y;
+    const float2 Pp = cmul(Dd, cconj(post[k]));
+    float2 zk, zm;
+    zk.x = Aa.x - Pp.y; zk.y = Aa.y + Pp.x;
+    zm.x = Aa.x + Pp.y; zm.y = -(Aa.y - Pp.x);
+    buf[L::at(k, row)] = zk;
+    if (k != 0 && MM - k != k) buf[L::at(MM - k, row)] = zm;
+  }
+}
+
+template <typename TI, int M, int MC, int RX>
+__global__ void __launch_bounds__(256) k_restrict_fx2(long long rows, const TI *__restrict__ in, float s,
+                                                      const float2 *__restrict__ post, const float2 *__restrict__ twg,
+                                                      const float2 *__restrict__ postc,
+                                                      const float2 *__restrict__ twcg, float *__restrict__ out) {
+  using V = float2;
+  using Lay = LayRow<M, Split<M>::R2>;
+  using LayC = LayRow<MC, Split<MC>::R2>;
+  using Q = typename Quad<TI>::type;
+  static_assert(MC < M && fx_buf<MC, RX>() <= fx_buf<M, RX>(), "coarse row tile must fit the fine one");
+  constexpr int N0 = 2 * M, Nc = 2 * MC, K = MC, K1 = MC + 1;
+  constexpr int PER = M / 2, CNT = (RX * PER + 255) / 256;
+  constexpr int PC = MC / 2;  // output float4 per row
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V *tw = reinterpret_cast<V *>(smem_raw);
+  V *buf = tw + M;
+  V *X = buf + fx_buf<M, RX>();
+  V *twc = X + RX * K1;
+  const int tid = threadIdx.x;
+  const long long nbat = (rows + RX - 1) / RX;
+  const float inv_n0 = 1.0f / (float)N0;
+  long long bat = blockIdx.x;
+  Q ra[CNT];
+#define FX2_LOAD_ROWS(BAT)                                                                          \
+  {                                                                                                 \
+    const long long r0 = (BAT) * RX;                                                                \
+    _Pragma("unroll") for (int it = 0; it < CNT; ++it) {                                            \
+      const int e = tid + it * 256;                                                                 \
+      const int row = e / PER, jj = (e % PER) * 2;                                                  \
+      if (e < RX * PER && r0 + row < rows) ra[it] = *reinterpret_cast<const Q *>(in + (r0 + row) * N0 + 2 * jj); \
+    }                                                                                               \
+  }
+  if (bat < nbat) FX2_LOAD_ROWS(bat)
+  for (int q = tid; q < M; q += 256) tw[q] = twg[q];
+  for (int q = tid; q < MC; q += 256) twc[q] = twcg[q];
+  for (; bat < nbat; bat += gridDim.x) {
+    const long long row0 = bat * RX;
+#pragma unroll
+    for (int it = 0; it < CNT; ++it) {
+      const int e = tid + it * 256;
+      if (e >= RX * PER) break;
+      const int row = e / PER, jj = (e % PER) * 2;
+      V a = make_float2(0.f, 0.f), b = a;
+      if (row0 + row < rows) {
+        Quad<TI>::split(ra[it], a, b);
+        a.x *= s; a.y *= s; b.x *= s; b.y *= s;
+      }
+      buf[Lay::at(jj, row)] = a;
+      buf[Lay::at(jj + 1, row)] = b;
+    }
+    if (bat + gridDim.x < nbat) FX2_LOAD_ROWS(bat + gridDim.x)
+    __syncthreads();
+    fft2<M, RX, 256, false, false, Lay>(buf, tw);
+    for (int e = tid; e < RX * K1; e += 256) {
+      const int row = e / K1, k = e - row * K1;
+      const V zk = buf[Lay::at(k, row)];
+      const V zm = buf[Lay::at(k == 0 ? 0 : M - k, row)];
+      V E, O;
+      E.x = (zk.x + zm.x) * 0.5f;
+      E.y = (zk.y - zm.y) * 0.5f;
+      O.x = (zk.y + zm.y) * 0.5f;
+      O.y = -(zk.x - zm.x) * 0.5f;
+      X[row * K1 + k] = cadd(E, cmul(post[k], O));
+    }
+    __syncthreads();
+    fx_pack_c2r<MC, RX, LayC>(X, K, K1, postc, buf);
+    __syncthreads();
+    fft2<MC, RX, 256, true, false, LayC>(buf, twc);
+    for (int e = tid; e < RX * PC; e += 256) {
+      const int row = e / PC, jj = (e - row * PC) * 2;
+      if (row0 + row >= rows) continue;
+      const V za = buf[LayC::at(jj, row)], zb = buf[LayC::at(jj + 1, row)];
+      *reinterpret_cast<float4 *>(out + (row0 + row) * Nc + 2 * jj) =
+          make_float4(za.x * inv_n0, za.y * inv_n0, zb.x * inv_n0, zb.y * inv_n0);
+    }
+    __syncthreads();
+  }
+#undef FX2_LOAD_ROWS
+}
+
+template <typename TO, typename TR, int M, int MC, int RX>
+__global__ void __launch_bounds__(256) k_prolong_fx2(long long rows, const float *__restrict__ y,
+                                                     const float2 *__restrict__ post, const float2 *__restrict__ twg,
+                                                     const float2 *__restrict__ postc,
+                                                     const float2 *__restrict__ twcg, const TR *__restrict__ r,
+                                                     double s, TO *__restrict__ out) {
+  using V = float2;
+  using Lay = LayRow<M, Split<M>::R2>;
+  using LayC = LayRow<MC, Split<MC>::R2>;
+  using QR = typename Quad<TR>::type;
+  static_assert(MC < M && fx_buf<MC, RX>() <= fx_buf<M, RX>(), "coarse row tile must fit the fine one");
+  constexpr int N0 = 2 * M, Nc = 2 * MC, K = MC, K1 = MC + 1;
+  constexpr int PER = M / 2, CNT = (RX * PER + 255) / 256;
+  constexpr int YC = (RX * MC + 255) / 256;  // coarse pairs per thread
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V *tw = reinterpret_cast<V *>(smem_raw);
+  V *buf = tw + M;
+  V *X = buf + fx_buf<M, RX>();
+  V *twc = X + RX * K1;
+  const int tid = threadIdx.x;
+  const long long nbat = (rows + RX - 1) / RX;
+  const float fk = 1.0f / (float)Nc;
+  long long bat = blockIdx.x;
+  QR rr[CNT], rn[CNT];
+  V yv[YC];
+#define FX2_LOAD(BAT, RR)                                                                           \
+  {                                                                                                 \
+    const long long r0 = (BAT) * RX;                                                                \
+    _Pragma("unroll") for (int it = 0; it < CNT; ++it) {                                            \
+      const int e = tid + it * 256;                                                                 \
+      const int row = e / PER, jj = (e % PER) * 2;                                                  \
+      if (e < RX * PER && r0 + row < rows) RR[it] = *reinterpret_cast<const QR *>(r + (r0 + row) * N0 + 2 * jj); \
+    }                                                                                               \
+    _Pragma("unroll") for (int q = 0; q < YC; ++q) {                                                \
+      const int e = tid + q * 256;                                                                  \
+      yv[q] = (e < RX * MC && r0 + e / MC < rows) ? *reinterpret_cast<const float2 *>(y + r0 * Nc + 2 * e) \
+                                                 : make_float2(0.f, 0.f);                          \
+    }                                                                                               \
+  }
+  if (bat < nbat) FX2_LOAD(bat, rr)
+  for (int q = tid; q < M; q += 256) tw[q] = twg[q];
+  for (int q = tid; q < MC; q += 256) twc[q] = twcg[q];
+  for (; bat < nbat; bat += gridDim.x) {
+    const long long row0 = bat * RX;
+#pragma unroll
+    for (int q = 0; q < YC; ++q) {
+      const int e = tid + q * 256;
+      if (e < RX * MC) buf[LayC::at(e % MC, e / MC)] = yv[q];
+    }
+    const bool more = bat + gridDim.x < nbat;
+    if (more) FX2_LOAD(bat + gridDim.x, rn)
+    __syncthreads();
+    fft2<MC, RX, 256, false, false, LayC>(buf, twc);
+    // untangle to the Nc-point r2c, weights f_k (1/Nc, half at the Nyquist K)
+    for (int e = tid; e < RX * K1; e += 256) {
+      const int row = e / K1, k = e - row * K1;
+      V xk;
+      if (k == K) {
+        const V z0 = buf[LayC::at(0, row)];
+        xk = make_float2((z0.x - z0.y) * 0.5f * fk, 0.f);
+      } else {
+        const V zk = buf[LayC::at(k, row)];
+        const V zm = buf[LayC::at(k == 0 ? 0 : MC - k, row)];
+        V E, O;
+        E.x = (zk.x + zm.x) * 0.5f;
+        E.y = (zk.y - zm.y) * 0.5f;
+        O.x = (zk.y + zm.y) * 0.5f;
+        O.y = -(zk.x - zm.x) * 0.5f;
+        xk = cadd(E, cmul(postc[k], O));
+        xk.x *= fk; xk.y *= fk;
+      }
+      X[row * K1 + k] = xk;
+    }
+    __syncthreads();
+    fx_pack_c2r<M, RX, Lay>(X, K, K1, post, buf);
+    __syncthreads();
+    fft2<M, RX, 256, true, false, Lay>(buf, tw);
+#pragma unroll
+    for (int it = 0; it < CNT; ++it) {
+      const int e = tid + it * 256;
+      if (e >= RX * PER) break;
+      const int row = e / PER, jj = (e % PER) * 2;
+      if (row0 + row >= rows) continue;
+      V ra, rb;
+      Quad<TR>::split(rr[it], ra, rb);
+      const V za = buf[Lay::at(jj, row)], zb = buf[Lay::at(jj + 1, row)];
+      TO *o = out + (row0 + row) * N0 + 2 * jj;
+      const TR *rx = r + (row0 + row) * N0 + 2 * jj;
+      if (sizeof(TR) == 8) {
+        o[0] = (TO)((double)za.x - s * (double)rx[0]);
+        o[1] = (TO)((double)za.y - s * (double)rx[1]);
+        o[2] = (TO)((double)zb.x - s * (double)rx[2]);
+        o[3] = (TO)((double)zb.y - s * (double)rx[3]);
+      } else {
+        const float sf = (float)s;
+        o[0] = (TO)(za.x - sf * ra.x);
+        o[1] = (TO)(za.y - sf * ra.y);
+        o[2] = (TO)(zb.x - sf * rb.x);
+        o[3] = (TO)(zb.y - sf * rb.y);
+      }
+    }
+    if (more) {
+#pragma unroll
+      for (int it = 0; it < CNT; ++it) rr[it] = rn[it];
+    }
+    __syncthreads();
+  }
+#undef FX2_LOAD
+}
+
+}  // namespace rism

@@ -165,12 +165,13 @@ def test_preconditioned_solve_reaches_the_root(fixture_loader, name, precision):
 @pytest.mark.parametrize("N, L", [((512, 48, 48), (48.0, 4.5, 4.5)), ((256, 48, 48), (24.0, 4.5, 4.5))])
 def test_fft_transfers_match_dense_long_rows(fixture_loader, N, L, monkeypatch):
     """256- and 128-point half rows: the preconditioner with the FFT x
-    transfers equals the one with the dense transfer tiles."""
+    transfers (both sides by FFT, and the coarse side by table product,
+    RISM3D_DENSE_TRANSFERS=2) equals the one with the dense transfer tiles."""
     meta, arr = fixture_loader("synth6_kh_n32")
     s = settings_of(meta, N=list(N), L=list(L))
     rng = np.random.default_rng(9)
     out = []
-    for dense in ("0", "1"):
+    for dense in ("0", "2", "1"):
         monkeypatch.setenv("RISM3D_DENSE_TRANSFERS", dense)
         ctx = RismContext(meta["solute"], meta["solvent"], s, arr["chi"])
         assert ctx.coarse_grid() is not None
@@ -179,4 +180,5 @@ def test_fft_transfers_match_dense_long_rows(fixture_loader, N, L, monkeypatch):
             v = to_dev(rng.standard_normal(ctx.shape))
         out.append(ctx.precondition(T, v).cpu().numpy())
         ctx.close()
-    assert np.max(np.abs(out[0] - out[1])) < 1e-4 * np.max(np.abs(out[1]))
+    for z in out[:2]:
+        assert np.max(np.abs(z - out[2])) < 1e-4 * np.max(np.abs(out[2]))
