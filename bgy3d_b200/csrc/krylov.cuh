@@ -23,36 +23,63 @@ template <typename T> struct Wide;
 template <> struct Wide<float> { using type = float4; static constexpr int n = 4; };
 template <> struct Wide<double> { using type = double2; static constexpr int n = 2; };
 
-// part[b * kVecMax + v] = sum over block b's range of w . V_v  (v < nv)
-template <typename T>
-__global__ void __launch_bounds__(256) k_mdotv(long long nw, const T *__restrict__ w, int nv, VecSet<T> vs,
-                                              double *__restrict__ part) {
+// The dot sweep of thread `i0` (stride `st`) over nw wide elements:
+// acc[v] += w . V_v for v < nv.  NVT (>= nv) bounds the accumulators held in
+// registers; for NVT <= 4 two strided elements are loaded before either is
+// used, so a thread keeps twice the bytes in flight.  The accumulation order
+// is that of the plain strided loop for every NVT.
+template <typename T, int NVT>
+__device__ __forceinline__ void mdot_sweep(long long nw, long long i0, long long st, const T *__restrict__ w, int nv,
+                                           const VecSet<T> &vs, double *acc) {
   using VT = typename Wide<T>::type;
   constexpr int WN = Wide<T>::n;
-  double acc[kVecMax];
+  constexpr int U = NVT <= 4 ? 2 : 1;
+  for (long long i = i0; i < nw; i += U * st) {
+    VT a[U], b[U][NVT];
 #pragma unroll
-  for (int v = 0; v < kVecMax; ++v) acc[v] = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += (long long)gridDim.x * blockDim.x) {
-    const VT a = reinterpret_cast<const VT *>(w)[i];
-    const T *ar = reinterpret_cast<const T *>(&a);
+    for (int u = 0; u < U; ++u) {
+      const long long iu = i + u * st;
+      if (iu < nw) {
+        a[u] = reinterpret_cast<const VT *>(w)[iu];
 #pragma unroll
-    for (int v = 0; v < kVecMax; ++v) {
-      if (v < nv) {
-        const VT b = reinterpret_cast<const VT *>(vs.p[v])[i];
-        const T *br = reinterpret_cast<const T *>(&b);
-        // products in the basis precision, one conversion per vector load
-        // (float -> double conversions would otherwise bound the kernel)
-        T s = T(0);
+        for (int v = 0; v < NVT; ++v)
+          if (v < nv) b[u][v] = reinterpret_cast<const VT *>(vs.p[v])[iu];
+      }
+    }
 #pragma unroll
-        for (int q = 0; q < WN; ++q) s += ar[q] * br[q];
-        acc[v] += (double)s;
+    for (int u = 0; u < U; ++u) {
+      if (i + u * st < nw) {
+        const T *ar = reinterpret_cast<const T *>(&a[u]);
+#pragma unroll
+        for (int v = 0; v < NVT; ++v) {
+          if (v < nv) {
+            const T *br = reinterpret_cast<const T *>(&b[u][v]);
+            // products in the basis precision, one conversion per vector load
+            // (float -> double conversions would otherwise bound the kernel)
+            T s = T(0);
+#pragma unroll
+            for (int q = 0; q < WN; ++q) s += ar[q] * br[q];
+            acc[v] += (double)s;
+          }
+        }
       }
     }
   }
-  __shared__ double sm[kVecMax][8];
+}
+
+// part[b * kVecMax + v] = sum over block b's range of w . V_v  (v < nv <= NVT)
+template <typename T, int NVT = kVecMax>
+__global__ void __launch_bounds__(256) k_mdotv(long long nw, const T *__restrict__ w, int nv, VecSet<T> vs,
+                                              double *__restrict__ part) {
+  double acc[NVT];
+#pragma unroll
+  for (int v = 0; v < NVT; ++v) acc[v] = 0.0;
+  mdot_sweep<T, NVT>(nw, (long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x, w, nv,
+                     vs, acc);
+  __shared__ double sm[NVT][8];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-  for (int v = 0; v < kVecMax; ++v) {
+  for (int v = 0; v < NVT; ++v) {
     if (v < nv) {
       double a = acc[v];
       for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
@@ -156,35 +183,20 @@ __global__ void k_scale_norm(long long n, T *__restrict__ w, const double *__res
 // replay) sums the block partials in a fixed order.
 //
 // k_mdot_red: h[v] = w . V_v for v < nv.
-template <typename T>
+template <typename T, int NVT = kVecMax>
 __global__ void __launch_bounds__(256) k_mdot_red(long long nw, const T *__restrict__ w, int nv, VecSet<T> vs,
                                                  double *__restrict__ part, unsigned *__restrict__ ticket,
                                                  double *__restrict__ h) {
-  using VT = typename Wide<T>::type;
-  constexpr int WN = Wide<T>::n;
-  double acc[kVecMax];
+  double acc[NVT];
 #pragma unroll
-  for (int v = 0; v < kVecMax; ++v) acc[v] = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += (long long)gridDim.x * blockDim.x) {
-    const VT a = reinterpret_cast<const VT *>(w)[i];
-    const T *ar = reinterpret_cast<const T *>(&a);
-#pragma unroll
-    for (int v = 0; v < kVecMax; ++v) {
-      if (v < nv) {
-        const VT b = reinterpret_cast<const VT *>(vs.p[v])[i];
-        const T *br = reinterpret_cast<const T *>(&b);
-        T s = T(0);
-#pragma unroll
-        for (int q = 0; q < WN; ++q) s += ar[q] * br[q];
-        acc[v] += (double)s;
-      }
-    }
-  }
-  __shared__ double sm[kVecMax][8];
+  for (int v = 0; v < NVT; ++v) acc[v] = 0.0;
+  mdot_sweep<T, NVT>(nw, (long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x, w, nv,
+                     vs, acc);
+  __shared__ double sm[NVT][8];
   __shared__ bool last;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-  for (int v = 0; v < kVecMax; ++v) {
+  for (int v = 0; v < NVT; ++v) {
     if (v < nv) {
       double a = acc[v];
       for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
@@ -322,6 +334,28 @@ __global__ static void k_arnoldi_lsq(int k, const double *__restrict__ H, const 
     y[i] = R[i][i] != 0.0 ? s / R[i][i] : 0.0;
   }
   if (k > 0) y[0] += *beta;
+}
+
+// Launch of the dot sweeps with the smallest accumulator bound NVT >= nv.
+template <typename T>
+void launch_mdotv(unsigned grid, cudaStream_t st, long long nw, const T *w, int nv, const VecSet<T> &vs,
+                  double *part) {
+  if (nv <= 1) k_mdotv<T, 1><<<grid, 256, 0, st>>>(nw, w, nv, vs, part);
+  else if (nv <= 2) k_mdotv<T, 2><<<grid, 256, 0, st>>>(nw, w, nv, vs, part);
+  else if (nv <= 4) k_mdotv<T, 4><<<grid, 256, 0, st>>>(nw, w, nv, vs, part);
+  else if (nv <= 8) k_mdotv<T, 8><<<grid, 256, 0, st>>>(nw, w, nv, vs, part);
+  else if (nv <= 16) k_mdotv<T, 16><<<grid, 256, 0, st>>>(nw, w, nv, vs, part);
+  else k_mdotv<T, kVecMax><<<grid, 256, 0, st>>>(nw, w, nv, vs, part);
+}
+template <typename T>
+void launch_mdot_red(unsigned grid, cudaStream_t st, long long nw, const T *w, int nv, const VecSet<T> &vs,
+                     double *part, unsigned *ticket, double *h) {
+  if (nv <= 1) k_mdot_red<T, 1><<<grid, 256, 0, st>>>(nw, w, nv, vs, part, ticket, h);
+  else if (nv <= 2) k_mdot_red<T, 2><<<grid, 256, 0, st>>>(nw, w, nv, vs, part, ticket, h);
+  else if (nv <= 4) k_mdot_red<T, 4><<<grid, 256, 0, st>>>(nw, w, nv, vs, part, ticket, h);
+  else if (nv <= 8) k_mdot_red<T, 8><<<grid, 256, 0, st>>>(nw, w, nv, vs, part, ticket, h);
+  else if (nv <= 16) k_mdot_red<T, 16><<<grid, 256, 0, st>>>(nw, w, nv, vs, part, ticket, h);
+  else k_mdot_red<T, kVecMax><<<grid, 256, 0, st>>>(nw, w, nv, vs, part, ticket, h);
 }
 
 }  // namespace rism

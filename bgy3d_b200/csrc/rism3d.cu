@@ -662,7 +662,7 @@ void mdot(rism3d_ctx *c, const T *w, double ws, const std::vector<VecRef<T>> &V,
     const int k = std::min(kVecMax, nv - base);
     VecSet<T> vs{};
     for (int i = 0; i < kVecMax; ++i) vs.p[i] = V[base + (i < k ? i : 0)].p;
-    k_mdotv<T><<<G, 256, 0, c->stream>>>(nw, w, k, vs, c->dpart);
+    launch_mdotv<T>(G, c->stream, nw, w, k, vs, c->dpart);
     CKL();
     k_colsum<<<1, kVecMax * 8, 0, c->stream>>>(G, kVecMax, k, c->dpart, c->dres + base);
     CKL();
@@ -1028,7 +1028,7 @@ void coarse_solve_dev(rism3d_ctx *c, int k) {
     for (int i = 0; i < kVecMax; ++i) vs.p[i] = B[i <= j ? i : 0];
     double *h = H + (size_t)j * (k + 1);
     // classical Gram-Schmidt, each sweep with its reduction fused in
-    k_mdot_red<float><<<G, 256, 0, st>>>(nw, B[j + 1], j + 1, vs, cc->dpart, c->cg_ticket, h);
+    launch_mdot_red<float>(G, st, nw, B[j + 1], j + 1, vs, cc->dpart, c->cg_ticket, h);
     k_maxpy_red<float><<<G, 256, 0, st>>>(nw, B[j + 1], j + 1, vs, h, cc->dpart, c->cg_ticket, h + j + 1);
     k_scale_by<float><<<gv, 256, 0, st>>>(cc->nvec, B[j + 1], h + j + 1);
     CKL();
