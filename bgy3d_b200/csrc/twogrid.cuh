@@ -240,7 +240,9 @@ __global__ void __launch_bounds__(kAxThreads) k_transfer_axis_j(int outer, int n
   float acc[J];
 #pragma unroll
   for (int jj = 0; jj < J; ++jj) acc[jj] = 0.f;
-#pragma unroll 2
+  // 8 strided input loads in flight per thread (the sweep is bound by their
+  // latency, not by the FMAs)
+#pragma unroll 8
   for (int k = 0; k < n_in; ++k) {
     const float v = src[(long long)k * inner];
     const float4 *a = reinterpret_cast<const float4 *>(&AtJ[k * J]);

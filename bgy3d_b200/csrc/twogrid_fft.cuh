@@ -407,8 +407,11 @@ __global__ void __launch_bounds__(256) k_restrict_fx2(long long rows, const TI *
 #undef FX2_LOAD_ROWS
 }
 
+// 128-point half rows (the 256^3 grid) at 3 CTAs per SM: at the compiler's
+// unbounded choice of 128 registers only 2 fit; the bound costs a few spilled
+// words there (more at 256-point rows, which keep the unbounded choice)
 template <typename TO, typename TR, int M, int MC, int RX>
-__global__ void __launch_bounds__(256) k_prolong_fx2(long long rows, const float *__restrict__ y,
+__global__ void __launch_bounds__(256, M == 128 ? 3 : 1) k_prolong_fx2(long long rows, const float *__restrict__ y,
                                                      const float2 *__restrict__ post, const float2 *__restrict__ twg,
                                                      const float2 *__restrict__ postc,
                                                      const float2 *__restrict__ twcg, const TR *__restrict__ r,
@@ -493,19 +496,27 @@ __global__ void __launch_bounds__(256) k_prolong_fx2(long long rows, const float
       V ra, rb;
       Quad<TR>::split(rr[it], ra, rb);
       const V za = buf[Lay::at(jj, row)], zb = buf[Lay::at(jj + 1, row)];
-      TO *o = out + (row0 + row) * N0 + 2 * jj;
+      TO *o = out + (row0 + row) * N0 + 2 * jj;  // 4 consecutive outputs, 4-element aligned
       const TR *rx = r + (row0 + row) * N0 + 2 * jj;
-      if (sizeof(TR) == 8) {
-        o[0] = (TO)((double)za.x - s * (double)rx[0]);
-        o[1] = (TO)((double)za.y - s * (double)rx[1]);
-        o[2] = (TO)((double)zb.x - s * (double)rx[2]);
-        o[3] = (TO)((double)zb.y - s * (double)rx[3]);
+      if constexpr (sizeof(TR) == 8) {
+        // the subtracted term in the output precision (r kept exact for FP64)
+        const double2 r01 = *reinterpret_cast<const double2 *>(rx), r23 = *reinterpret_cast<const double2 *>(rx + 2);
+        const double o0 = (double)za.x - s * r01.x, o1 = (double)za.y - s * r01.y;
+        const double o2 = (double)zb.x - s * r23.x, o3 = (double)zb.y - s * r23.y;
+        if constexpr (sizeof(TO) == 8) {
+          *reinterpret_cast<double2 *>(o) = make_double2(o0, o1);
+          *reinterpret_cast<double2 *>(o + 2) = make_double2(o2, o3);
+        } else {
+          o[0] = (TO)o0; o[1] = (TO)o1; o[2] = (TO)o2; o[3] = (TO)o3;
+        }
       } else {
         const float sf = (float)s;
-        o[0] = (TO)(za.x - sf * ra.x);
-        o[1] = (TO)(za.y - sf * ra.y);
-        o[2] = (TO)(zb.x - sf * rb.x);
-        o[3] = (TO)(zb.y - sf * rb.y);
+        const float o0 = za.x - sf * ra.x, o1 = za.y - sf * ra.y, o2 = zb.x - sf * rb.x, o3 = zb.y - sf * rb.y;
+        if constexpr (sizeof(TO) == 4) {
+          *reinterpret_cast<float4 *>(o) = make_float4(o0, o1, o2, o3);
+        } else {
+          o[0] = (TO)o0; o[1] = (TO)o1; o[2] = (TO)o2; o[3] = (TO)o3;
+        }
       }
     }
     if (more) {
