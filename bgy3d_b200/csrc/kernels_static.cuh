@@ -137,16 +137,12 @@ __global__ void __launch_bounds__(256) k_xinv_s(Geo g, const typename Cx<T>::typ
     if (e < RX * PER_ROW && row0 + row < rows_total)
       rin[it] = *reinterpret_cast<const VEC *>(In + sbase + (long long)(row0 + row) * g.N0 + 2 * jj);
   }
-#pragma unroll 2
-  for (int e = tid; e < RX * H; e += 256) {
+  // packed c2r input of element e = (row, k <= M/2) from X_k and X_{M-k}
+  auto pack = [&](int e, V xk, V xm) {
     const int row = e / H, k = e % H;
-    const int grow = row0 + row;
     V zk, zm;
     zk.x = zk.y = zm.x = zm.y = T(0);
-    if (grow < rows_total) {
-      const V *row_in = W + wbase + (long long)grow * g.Nhp;
-      V xk = row_in[k];
-      V xm = row_in[M - k];
+    if (row0 + row < rows_total) {
       if (k == 0) { xk.y = T(0); xm.y = T(0); }  // c2r reads only Re X_0, Re X_{N0/2}
       V Aa, D;
       Aa.x = xk.x + xm.x; Aa.y = xk.y - xm.y;
@@ -157,6 +153,55 @@ __global__ void __launch_bounds__(256) k_xinv_s(Geo g, const typename Cx<T>::typ
     }
     buf[Lay::at(k, row)] = zk;
     if (k != 0 && M - k != k) buf[Lay::at(M - k, row)] = zm;
+  };
+  auto ld = [&](int e, V &xk, V &xm) {
+    const int row = e / H, k = e % H;
+    if (row0 + row < rows_total) {
+      const V *row_in = W + wbase + (long long)(row0 + row) * g.Nhp;
+      xk = row_in[k];
+      xm = row_in[M - k];
+    } else {
+      xk.x = xk.y = xm.x = xm.y = T(0);
+    }
+  };
+  constexpr int CW = (RX * H + 255) / 256;
+  if constexpr (CW <= 6) {
+    // every (X_k, X_{M-k}) pair of this thread is loaded before the first is
+    // used: one memory latency per CTA instead of one per pair of iterations
+    // (longer rows keep the loop below: the registers would cost occupancy)
+    V xkv[CW], xmv[CW];
+#pragma unroll
+    for (int it = 0; it < CW; ++it) {
+      const int e = tid + it * 256;
+      if (e < RX * H) ld(e, xkv[it], xmv[it]);
+    }
+#pragma unroll
+    for (int it = 0; it < CW; ++it) {
+      const int e = tid + it * 256;
+      if (e < RX * H) pack(e, xkv[it], xmv[it]);
+    }
+  } else {
+#pragma unroll 2
+    for (int e = tid; e < RX * H; e += 256) {
+      const int row = e / H, k = e % H;
+      const int grow = row0 + row;
+      V zk, zm;
+      zk.x = zk.y = zm.x = zm.y = T(0);
+      if (grow < rows_total) {
+        const V *row_in = W + wbase + (long long)grow * g.Nhp;
+        V xk = row_in[k];
+        V xm = row_in[M - k];
+        if (k == 0) { xk.y = T(0); xm.y = T(0); }
+        V Aa, D;
+        Aa.x = xk.x + xm.x; Aa.y = xk.y - xm.y;
+        D.x = xk.x - xm.x;  D.y = xk.y + xm.y;
+        const V Pp = cmul(D, cconj(post[k]));
+        zk.x = Aa.x - Pp.y; zk.y = Aa.y + Pp.x;
+        zm.x = Aa.x + Pp.y; zm.y = -(Aa.y - Pp.x);
+      }
+      buf[Lay::at(k, row)] = zk;
+      if (k != 0 && M - k != k) buf[Lay::at(M - k, row)] = zm;
+    }
   }
   __syncthreads();
   fft2<M, RX, 256, true, false, Lay>(buf, tw);
