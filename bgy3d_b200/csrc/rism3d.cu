@@ -21,6 +21,7 @@
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <tuple>
 #include <vector>
@@ -2696,6 +2697,90 @@ int info_impl(rism3d_ctx *c, const double *T, rism3d_info_result *res, double *s
 }
 
 // One solve on a fresh context from host buffers (rism3d_solute_solve).
+// Device -> host copy of a large result into caller memory that is
+// pageable (a NumPy array, a PETSc Vec): the driver's pageable path runs
+// at a few GB/s there, the faults of untouched destination pages taken by
+// one thread.  Here two pinned chunks alternate: the DMA of chunk i runs
+// while host threads copy chunk i-1 out, splitting it so that the
+// destination's page faults are taken in parallel.  The pinned chunk pairs
+// come from a process-wide free list (one pair per concurrent caller,
+// 2 x kStageChunk bytes each, held until exit).  Copies below two chunks
+// take the plain cudaMemcpy.
+constexpr size_t kStageChunk = size_t(16) << 20;
+struct StagePair {
+  void *buf[2];
+};
+std::mutex g_stage_mu;
+std::vector<StagePair> g_stage_free;
+
+void d2h_large(void *dst, const void *src, size_t bytes, cudaStream_t st) {
+  if (bytes < 2 * kStageChunk) {
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return;
+  }
+  StagePair sp{{nullptr, nullptr}};
+  {
+    std::lock_guard<std::mutex> lk(g_stage_mu);
+    if (!g_stage_free.empty()) {
+      sp = g_stage_free.back();
+      g_stage_free.pop_back();
+    }
+  }
+  if (!sp.buf[0]) {
+    for (int b = 0; b < 2; ++b) CK(cudaHostAlloc(&sp.buf[b], kStageChunk, cudaHostAllocPortable));
+  }
+  struct Back {
+    StagePair sp;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    ~Back() {
+      for (auto e : ev)
+        if (e) cudaEventDestroy(e);
+      std::lock_guard<std::mutex> lk(g_stage_mu);
+      g_stage_free.push_back(sp);
+    }
+  } back{sp};
+  for (auto &e : back.ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int nthr = (int)std::max(1u, std::min(8u, hw ? hw : 1u));
+  // host copy of chunk `c` (bytes [off, off + len)) out of its staging buffer
+  auto drain = [&](size_t off, size_t len, const void *stage) {
+    const size_t slice = ((len / nthr) + 63) & ~size_t(63);
+    auto part = [=](size_t a, size_t b) {
+      std::memcpy(static_cast<char *>(dst) + off + a, static_cast<const char *>(stage) + a, b - a);
+    };
+    std::vector<std::thread> th;
+    for (int q = 1; q < nthr; ++q) {
+      const size_t a = std::min(len, q * slice), b = std::min(len, (q + 1) * slice);
+      if (a >= b) continue;
+      try {
+        th.emplace_back(part, a, b);
+      } catch (const std::system_error &) {  // no thread to be had: copy here
+        part(a, b);
+      }
+    }
+    part(0, std::min(len, slice));
+    for (auto &t : th) t.join();
+  };
+  const size_t nchunk = (bytes + kStageChunk - 1) / kStageChunk;
+  size_t prev_off = 0, prev_len = 0;
+  for (size_t c = 0; c <= nchunk; ++c) {
+    if (c < nchunk) {  // the buffer of chunk c was drained two steps ago
+      const size_t off = c * kStageChunk, len = std::min(kStageChunk, bytes - off);
+      CK(cudaMemcpyAsync(sp.buf[c & 1], static_cast<const char *>(src) + off, len, cudaMemcpyDeviceToHost, st));
+      CK(cudaEventRecord(back.ev[c & 1], st));
+    }
+    if (c > 0) {
+      CK(cudaEventSynchronize(back.ev[(c - 1) & 1]));
+      drain(prev_off, prev_len, sp.buf[(c - 1) & 1]);
+    }
+    if (c < nchunk) {
+      prev_off = c * kStageChunk;
+      prev_len = std::min(kStageChunk, bytes - prev_off);
+    }
+  }
+}
+
 int solve_on(rism3d_ctx *ctx, double *t_inout, double *g_out, rism3d_result *out) {
   const size_t bytes = sizeof(double) * ctx->nvec;
   double *T = dalloc<double>(ctx->nvec);
@@ -2708,8 +2793,8 @@ int solve_on(rism3d_ctx *ctx, double *t_inout, double *g_out, rism3d_result *out
   observables_impl(ctx, T, g, &r);
   r.launches += 2;  // the observables' kernels
   r.status = st;
-  if (t_inout) CK(cudaMemcpy(t_inout, T, bytes, cudaMemcpyDeviceToHost));
-  if (g_out) CK(cudaMemcpy(g_out, g, bytes, cudaMemcpyDeviceToHost));
+  if (t_inout) d2h_large(t_inout, T, bytes, ctx->stream);
+  if (g_out) d2h_large(g_out, g, bytes, ctx->stream);
   if (out) *out = r;
   return st;
 }
