@@ -532,7 +532,7 @@ def run_ours(args, rank, world):
     if clocks:
         line["clocks"] = clocks
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args, sample_evals=1)
+        line["cpu_baseline"] = cpu_baseline(args)
     if world == 1 and not args.no_extras:
         extras = (("batch", lambda: run_batch_report(solvent, s, chi)),
                   ("gradient", lambda: run_gradient_report(solute, solvent, s, chi, ms / args.steps)),
@@ -546,53 +546,118 @@ def run_ours(args, rank, world):
     return line
 
 
-def cpu_sample(grid, sample_evals):
-    """Time sample_evals residual and Jacobian evaluations of the CPU
-    restatement at the full workload size; return seconds per solve."""
-    import os as _os
-    from oracle import hnc3d
+def host_threads():
+    """Host threads this process may run on (all of them are used)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_problem(grid, threads):
+    """The workload as the CPU restatement's Problem (built once); returns it
+    with its set-up time (field, chi and long-range tables)."""
     from oracle import closures as cl
+    from oracle import hnc3d
     solute, solvent, s, chi = workload(grid)
+    t0 = time.perf_counter()
     P = hnc3d.Problem((grid,) * 3, (2 * s["L"],) * 3, s["beta"], s["rho"], cl.KH, solvent, solute, chi,
-                      s["rmax"])
-    T = np.zeros((3, grid, grid, grid))
-    P.iterate_t1(T)  # warm the FFT plans
-    t0 = time.perf_counter()
-    for _ in range(sample_evals):
-        F = P.iterate_t1(T)
-    tf = (time.perf_counter() - t0) / sample_evals
-    t0 = time.perf_counter()
-    for _ in range(sample_evals):
-        P.jacobian_t1(T, F)
-    tj = (time.perf_counter() - t0) / sample_evals
-    per_solve = FP64_SOLVE_EVALS["f"] * tf + FP64_SOLVE_EVALS["jv"] * tj
-    # threads used: the FFTs run on hnc3d's worker pool, the rest is serial NumPy
-    return per_solve, tf, tj, min(hnc3d._WORKERS, _os.cpu_count() or 1)
+                      s["rmax"], threads=threads)
+    return P, time.perf_counter() - t0
 
 
-def cpu_baseline(args, sample_evals=1):
-    per_solve, tf, tj, cores = cpu_sample(args.grid, sample_evals)
-    return {"value": 1.0 / per_solve, "unit": "solves/s", "cores": cores, "kind": "port",
-            "sample": f"{sample_evals} iterate_t1 + {sample_evals} jacobian_t1 of the NumPy/SciPy restatement "
-                      f"at {args.grid}^3 ({tf:.2f} s + {tj:.2f} s), scaled by the {FP64_SOLVE_EVALS['f']} + "
-                      f"{FP64_SOLVE_EVALS['jv']} evaluations of one plain FP64 Newton-GMRES solve"}
+def cpu_evals(P):
+    """One bounded sample: one iterate_t1 and one jacobian_t1 of the CPU
+    restatement at the workload's size; returns their seconds."""
+    T = np.zeros((P.m, P.N[2], P.N[1], P.N[0]))
+    t0 = time.perf_counter()
+    F = P.iterate_t1(T)
+    tf = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    P.jacobian_t1(T, F)
+    return tf, time.perf_counter() - t0
+
+
+def per_solve_model(setup_s, tf, tj):
+    """Seconds of one plain FP64 solve: set-up plus the residual and Jacobian
+    evaluations of the reference's Newton-GMRES at this workload."""
+    return setup_s + FP64_SOLVE_EVALS["f"] * tf + FP64_SOLVE_EVALS["jv"] * tj
+
+
+def cpu_scaling_check(threads, grid=64):
+    """A complete plain FP64 Newton-GMRES solve (GMRES(30), rtol 1e-3,
+    backtracking) of the workload's solute at a small grid on the CPU
+    restatement, timed, against the evaluation-count model: the model holds
+    when the solve's time is its set-up plus its F and J.v evaluations."""
+    from oracle import newton
+    P, setup_s = cpu_problem(grid, threads)
+    cnt = {"f": 0, "jv": 0, "tf": 0.0, "tj": 0.0}
+
+    def F(x):
+        t0 = time.perf_counter()
+        r = P.iterate_t1(x)
+        cnt["tf"] += time.perf_counter() - t0
+        cnt["f"] += 1
+        return r
+
+    def J(x, v):
+        t0 = time.perf_counter()
+        r = P.jacobian_t1(x, v)
+        cnt["tj"] += time.perf_counter() - t0
+        cnt["jv"] += 1
+        return r
+
+    t0 = time.perf_counter()
+    newton.solve(F, np.zeros((P.m, grid, grid, grid)), jv=J, tol=SETTINGS["norm-tol"])
+    solve_s = time.perf_counter() - t0
+    tf, tj = cnt["tf"] / max(cnt["f"], 1), cnt["tj"] / max(cnt["jv"], 1)
+    model = setup_s + cnt["f"] * tf + cnt["jv"] * tj
+    return {"grid": grid, "f_evals": cnt["f"], "jv_evals": cnt["jv"], "measured_s": setup_s + solve_s,
+            "model_s": model, "measured_over_model": (setup_s + solve_s) / model}
+
+
+def cpu_baseline(args):
+    threads = host_threads()
+    P, setup_s = cpu_problem(args.grid, threads)
+    tf, tj = cpu_evals(P)
+    per_solve = per_solve_model(setup_s, tf, tj)
+    return {"value": 1.0 / per_solve, "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"NumPy/SciPy restatement of hnc3d.c on {threads} host threads at {args.grid}^3: set-up "
+                      f"{setup_s:.2f} s + {FP64_SOLVE_EVALS['f']} x iterate_t1 ({tf:.2f} s) + "
+                      f"{FP64_SOLVE_EVALS['jv']} x jacobian_t1 ({tj:.2f} s), the evaluations of one plain FP64 "
+                      f"Newton-GMRES solve; one F and one J.v timed"}
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference's algorithm
+    (the reference itself needs PETSc/FFTW/MPI/Guile, absent here) on all
+    host threads.  Built once; each step is one bounded sample (one F and
+    one J.v at the full size) scaled to a solve by the evaluation counts."""
+    threads = host_threads()
+    P, setup_s = cpu_problem(args.grid, threads)
     times = []
     for _ in range(args.warmup + args.steps):
-        per_solve, tf, tj, cores = cpu_sample(args.grid, 1)
-        times.append(per_solve)
+        tf, tj = cpu_evals(P)
+        times.append((tf, tj))
     t = times[args.warmup:]
-    value = len(t) / sum(t)
+    tf = sum(a for a, _ in t) / len(t)
+    tj = sum(b for _, b in t) / len(t)
+    per_solve = per_solve_model(setup_s, tf, tj)
+    value = 1.0 / per_solve
+    del P
+    check = cpu_scaling_check(threads)
+    sample = (f"per step one iterate_t1 + one jacobian_t1 of the NumPy/SciPy restatement of hnc3d.c at "
+              f"{args.grid}^3 on {threads} host threads (mean {tf:.3f} s + {tj:.3f} s over {len(t)} steps); a solve "
+              f"= set-up ({setup_s:.2f} s, once) + {FP64_SOLVE_EVALS['f']} F + {FP64_SOLVE_EVALS['jv']} J.v, the "
+              f"evaluations of the plain FP64 Newton-GMRES solve; model checked by a complete CPU solve at "
+              f"{check['grid']}^3 (measured / model = {check['measured_over_model']:.3f})")
     return {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * sum(t) / len(t), "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1e3 * per_solve, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
             "data": "synthetic (seeded solute, 1D-DRISM chi)", "config": config(args.grid, "fp64"),
-            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
-                             "sample": "per step: one iterate_t1 + one jacobian_t1 of the NumPy/SciPy "
-                                       "restatement of hnc3d.c (the reference needs PETSc/FFTW/MPI/Guile, "
-                                       "absent here), scaled by the evaluations of one FP64 Newton solve"},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "scaling_check": check,
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 

@@ -64,7 +64,8 @@ class Job(ctypes.Structure):
 class Grad(ctypes.Structure):
     _fields_ = [("dq", ctypes.POINTER(ctypes.c_double)), ("dsigma", ctypes.POINTER(ctypes.c_double)),
                 ("depsilon", ctypes.POINTER(ctypes.c_double)), ("dx", ctypes.POINTER(ctypes.c_double)),
-                ("adjoint_jv", ctypes.c_int), ("adjoint_resid", ctypes.c_double), ("seconds", ctypes.c_double)]
+                ("adjoint_jv", ctypes.c_int), ("adjoint_resid", ctypes.c_double), ("seconds", ctypes.c_double),
+                ("dx_reference", ctypes.POINTER(ctypes.c_double))]
 
 
 class SolventResult(ctypes.Structure):
@@ -96,6 +97,7 @@ EXPORTS = [
     "rism3d_solute_grad", "rism3d_gradient", "rism3d_jacobian_transpose_t1", "rism3d_ctx_set_solute",
     "rism3d_response", "rism3d_solvent_solve", "rism3d_solvent_ctx_create", "rism3d_ctx_create_chi3",
     "rism3d_solute_solve_chi3", "rism3d_info", "rism3d_moments", "rism3d_tile_shapes",
+    "rism3d_free_energy_gradient",
 ]
 
 _lib = None
@@ -170,6 +172,8 @@ def lib():
     L.rism3d_moments.restype = I
     L.rism3d_tile_shapes.argtypes = [V, P(I)]
     L.rism3d_tile_shapes.restype = I
+    L.rism3d_free_energy_gradient.argtypes = [V, V, P(D)]
+    L.rism3d_free_energy_gradient.restype = I
     _lib = L
     return L
 

@@ -179,6 +179,24 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
   }
   return false;
 }
+// Every thread of the CTA waits for phase `parity` of `bar`; the result is
+// CTA-uniform (one barrier with a vote replaces the barrier that follows the
+// wait anyway).  On a timeout thread 0 records `code` in *err and waits once
+// more, bounded, so that a transaction still in flight lands while the CTA
+// is resident; the whole CTA then leaves together.
+__device__ __forceinline__ bool cta_wait_tile(uint64_t *bar, uint32_t parity, uint32_t max_polls, int *err,
+                                              int code) {
+  const bool ok = mbar_wait(bar, parity, max_polls);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) {
+      atomicExch(err, code);
+      mbar_wait(bar, parity, max_polls);
+    }
+    __syncthreads();
+    return false;
+  }
+  return true;
+}
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1,
                                             int c2) {
   asm volatile(

@@ -287,6 +287,85 @@ static __global__ void k_field1(Geo g, double h0, double h1, double h2, double L
   }
 }
 
+// The reference's free-energy gradient, the `derivatives` output of
+// hnc3d_solute_solve (gradients / energy1, hnc3d.c:1665-1742, with field1,
+// bgy3d-solutes.c:381-468): de[u][dim] = rho h^3 sum_i sum_r g_i(r)
+// dv_i/dR_{u,dim}(r), g = c(t) + t + 1 and dv the LJ and FULL capped
+// Coulomb derivative of a unit displacement of site u (0 at r = 0, where
+// the reference takes no limit).  Block (blockIdx.x, blockIdx.y) sums sites
+// u = U blockIdx.y ... U blockIdx.y + U - 1 over its grid points:
+// part[(u * gridDim.x + blockIdx.x) * 3 + dim] (rho h^3 applied on the host).
+template <int U>
+static __global__ void __launch_bounds__(256) k_force_pair(Geo g, double h0, double h1, double h2, double L0,
+                                                           double L1, double L2, const SiteP *__restrict__ solvent,
+                                                           int n, const SiteP *__restrict__ solute,
+                                                           const double *__restrict__ t,
+                                                           const double *__restrict__ v, double beta, int closure,
+                                                           double *__restrict__ part) {
+  const int u0 = blockIdx.y * U;
+  const int m = g.m;
+  double acc[U][3];
+#pragma unroll
+  for (int k = 0; k < U; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.0;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.Nr;
+       p += (long long)gridDim.x * blockDim.x) {
+    const int i0 = (int)(p % g.N0);
+    const int i1 = (int)((p / g.N0) % g.N1);
+    const int i2 = (int)(p / ((long long)g.N0 * g.N1));
+    const double x = i0 * h0 - L0 / 2, y = i1 * h1 - L1 / 2, z = i2 * h2 - L2 / 2;
+    double gs[kMaxSites];
+#pragma unroll
+    for (int s = 0; s < kMaxSites; ++s) {
+      if (s < m) {
+        const long long o = (long long)s * g.Nr + p;
+        const double ts = t[o];
+        gs[s] = closure_c<double>(closure, beta * v[o], ts) + ts + 1.0;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const int u = u0 + k;
+      if (u >= n) break;
+      const SiteP b = solute[u];
+      const double ab[3] = {x - b.x, y - b.y, z - b.z};
+      const double r = sqrt(ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2]);
+      if (!(r > 0.0)) continue;
+      double f = 0.0;
+#pragma unroll
+      for (int s = 0; s < kMaxSites; ++s) {
+        if (s < m) {
+          const SiteP a = solvent[s];
+          const double eab = sqrt(a.epsilon * b.epsilon), sab = 0.5 * (a.sigma + b.sigma);
+          const double qab = a.charge * b.charge * kEps0Inv;
+          f += gs[s] * ((eab / sab) * ljcap1(r / sab) + qab * kG * kG * ccap1(kG * r));
+        }
+      }
+      // drab = -ab[dim] / r
+#pragma unroll
+      for (int d = 0; d < 3; ++d) acc[k][d] -= f * (ab[d] / r);
+    }
+  }
+  __shared__ double sm[U * 3][8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < U; ++k)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      double a = acc[k][d];
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+      if (lane == 0) sm[3 * k + d][wid] = a;
+    }
+  __syncthreads();
+  if (threadIdx.x < U * 3) {
+    const int u = u0 + threadIdx.x / 3;
+    if (u < n) {
+      double a = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a += sm[threadIdx.x][w];
+      part[((long long)u * gridDim.x + blockIdx.x) * 3 + threadIdx.x % 3] = a;
+    }
+  }
+}
+
 // out = d + 1 (the closure's dh/dx, the slope the flagged Jacobian applies).
 static __global__ void k_shift1(long long n, const double *__restrict__ d, double *__restrict__ out) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)

@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(256) k_xfwd(Geo g, AxisPlan px, int RX, const 
                                              const typename Cx<T>::type *__restrict__ post) {
   using V = typename Cx<T>::type;
   using P2 = typename Vec2<T>::type;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   V *tw = reinterpret_cast<V *>(smem_raw);
   V *buf = tw + px.n;
   const int M = g.M;
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(256) k_xfwd(Geo g, AxisPlan px, int RX, const 
 template <typename T, bool INV, int B>
 __global__ void __launch_bounds__(256) k_y(Geo g, AxisPlan py, typename Cx<T>::type *__restrict__ W) {
   using V = typename Cx<T>::type;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   V *tw = reinterpret_cast<V *>(smem_raw);
   V *buf = tw + py.n;
   const int tid = threadIdx.x, nthr = blockDim.x;
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(256) k_z(Geo g, AxisPlan pz, typename Cx<T>::t
                                           ZParams<T> zp) {
   using V = typename Cx<T>::type;
   using P2 = typename Vec2<T>::type;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   V *tw = reinterpret_cast<V *>(smem_raw);
   V *buf = tw + pz.n;
   const int tid = threadIdx.x, nthr = blockDim.x;
@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(256) k_xinv(Geo g, AxisPlan px, int RX,
                                              NormPartial *__restrict__ part) {
   using V = typename Cx<T>::type;
   using P2 = typename Vec2<T>::type;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   V *tw = reinterpret_cast<V *>(smem_raw);
   V *buf = tw + px.n;
   const int M = g.M;

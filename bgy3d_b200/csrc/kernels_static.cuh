@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(256) k_xfwd_s(Geo g, const T *__restrict__ A, 
   using Lay = LayRow<M, Split<M>::R2>;
   constexpr int VW = VecW<T>::n;
   using VEC = typename VecW<T>::vec;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   V *tw = reinterpret_cast<V *>(smem_raw);
   V *buf = tw + M;
   const int tid = threadIdx.x;
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(256) k_xinv_s(Geo g, const typename Cx<T>::typ
   using Lay = LayRow<M, Split<M>::R2>;
   constexpr int VW = VecW<T>::n;
   using VEC = typename VecW<T>::vec;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   V *tw = reinterpret_cast<V *>(smem_raw);
   V *buf = tw + M;
   const int tid = threadIdx.x;
@@ -260,11 +260,7 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_y_s(Geo g, const __grid_co
     for (int c = 0; c < N; c += kTmaRows) tma_load_3d(buf + c * B, &tm, bar, 2 * kx0, c, site * g.N2 + z);
   }
   for (int q = tid; q < N; q += NTHR) tw[q] = twg[q];
-  if (!mbar_wait(bar, 0, kMbarPolls)) {
-    if (tid == 0) atomicExch(err, 1);
-    return;
-  }
-  __syncthreads();
+  if (!cta_wait_tile(bar, 0, kMbarPolls, err, 1)) return;
   fft2<N, B, NTHR, INV, true, LayCol<N, B>>(buf, tw);
   fence_proxy_async();
   __syncthreads();
@@ -390,11 +386,7 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_z_s(Geo g, const __grid_co
       for (int c = 0; c < N; c += kTmaRows) tma_load_3d(buf + s * N * B + c * B, &tm, bar, 2 * kx0, y, s * g.N2 + c);
   }
   for (int q = tid; q < N; q += NTHR) tw[q] = twg[q];
-  if (!mbar_wait(bar, 0, kMbarPolls)) {
-    if (tid == 0) atomicExch(err, 2);
-    return;
-  }
-  __syncthreads();
+  if (!cta_wait_tile(bar, 0, kMbarPolls, err, 2)) return;
   z_tile<T, MODE, N, B, MS>(g, buf, tw, zp, kx0, y);
   fence_proxy_async();
   __syncthreads();
@@ -455,14 +447,20 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_z_sp(Geo g, const __grid_c
           tma_load_3d(bufs[cur ^ 1] + s * N * B + c * B, &tm, &bar[cur ^ 1], 2 * (tn % nkx) * B, tn / nkx,
                       s * g.N2 + c);
     }
-    if (!mbar_wait(&bar[cur], (uint32_t)((it >> 1) & 1), kMbarPolls)) {
+    const bool ok = mbar_wait(&bar[cur], (uint32_t)((it >> 1) & 1), kMbarPolls);
+    if (__syncthreads_or(!ok)) {
+      // a CTA-uniform exit: both buffers' loads (this tile's and the
+      // prefetch of the next) get one more bounded wait, and the stores
+      // drain, before the CTA leaves
       if (tid == 0) {
         atomicExch(err, 2);
+        mbar_wait(&bar[cur], (uint32_t)((it >> 1) & 1), kMbarPolls);
+        if (tn < ntile) mbar_wait(&bar[cur ^ 1], (uint32_t)(((it + 1) >> 1) & 1), kMbarPolls);
         tma_wait0();
       }
+      __syncthreads();
       return;
     }
-    __syncthreads();
     const int kx0 = (t % nkx) * B, y = t / nkx;
     z_tile<T, MODE, N, B, MS>(g, bufs[cur], tw, zp, kx0, y);
     fence_proxy_async();

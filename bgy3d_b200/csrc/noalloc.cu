@@ -29,6 +29,10 @@
 
 using namespace rism;
 
+namespace rism {
+void set_last_error(const std::string &msg);  // rism3d.cu: the message of rism3d_last_error()
+}
+
 namespace {
 
 constexpr size_t kNoallocScratchBytes = size_t(32) << 20;
@@ -39,21 +43,28 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratch
 // current.  In host code the symbol is only a stand-in, never an address.
 std::mutex g_mu;
 void *g_addr[64] = {nullptr};
-thread_local std::string g_msg;
+
+// Records a failed CUDA call for rism3d_last_error() and returns the code.
+int cuda_fail(const char *what, cudaError_t e) {
+  set_last_error(std::string("rism3d_jacobian_apply_noalloc: ") + what + ": " + cudaGetErrorString(e));
+  return RISM3D_ERR_CUDA;
+}
 
 int setup(int dev, void **out) {
   std::lock_guard<std::mutex> lk(g_mu);
-  if (dev < 0 || dev >= 64) return RISM3D_ERR_ARG;
+  if (dev < 0 || dev >= 64) {
+    set_last_error("rism3d_jacobian_apply_noalloc: device ordinal beyond 63");
+    return RISM3D_ERR_ARG;
+  }
   if (!g_addr[dev]) {
     void *p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
-      g_msg = "cudaGetSymbolAddress of the scratch array failed";
-      return RISM3D_ERR_CUDA;
-    }
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail("cudaGetSymbolAddress of the scratch array", e);
+    if (!p) return cuda_fail("cudaGetSymbolAddress of the scratch array", cudaErrorInvalidSymbol);
     // the passes may use more than 48 KB of dynamic shared memory
     int optin = 0;
-    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
-      return RISM3D_ERR_CUDA;
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return cuda_fail("cudaDeviceGetAttribute", e);
     const void *fns[] = {(const void *)k_xfwd<double, MODE_J>, (const void *)k_xinv<double>,
                          (const void *)k_y<double, false, 16>, (const void *)k_y<double, true, 16>,
                          (const void *)k_y<double, false, 8>,  (const void *)k_y<double, true, 8>,
@@ -62,10 +73,10 @@ int setup(int dev, void **out) {
                          (const void *)k_z<double, MODE_J, 4>};
     for (const void *f : fns) {
       cudaFuncAttributes fa{};
-      if (cudaFuncGetAttributes(&fa, f) != cudaSuccess) return RISM3D_ERR_CUDA;
-      if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes) !=
-          cudaSuccess)
-        return RISM3D_ERR_CUDA;
+      e = cudaFuncGetAttributes(&fa, f);
+      if (e != cudaSuccess) return cuda_fail("cudaFuncGetAttributes", e);
+      e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+      if (e != cudaSuccess) return cuda_fail("cudaFuncSetAttribute", e);
     }
     g_addr[dev] = p;
   }
@@ -106,10 +117,15 @@ size_t up256(size_t b) { return (b + 255) & ~size_t(255); }
 
 extern "C" int rism3d_jacobian_apply_noalloc(const rism3d_problem *pd, int m, const double *chi, const double *d,
                                              const double *dT, double *JdT) {
-  if (!pd || !chi || !d || !dT || !JdT || m < 1 || m > kMaxSites || pd->nrad < 4 || !(pd->rmax > 0))
+  if (!pd || !chi || !d || !dT || !JdT || m < 1 || m > kMaxSites || pd->nrad < 4 || !(pd->rmax > 0)) {
+    set_last_error("rism3d_jacobian_apply_noalloc: NULL pointer, site count or chi table out of range");
     return RISM3D_ERR_ARG;
+  }
   for (int a = 0; a < 3; ++a)
-    if (!is_2a3b_even(pd->N[a]) || !(pd->L[a] > 0)) return RISM3D_ERR_ARG;
+    if (!is_2a3b_even(pd->N[a]) || !(pd->L[a] > 0)) {
+      set_last_error("rism3d_jacobian_apply_noalloc: grid sizes must be even 2^a 3^b in 8..512, box edges > 0");
+      return RISM3D_ERR_ARG;
+    }
   Geo g{};
   g.N0 = pd->N[0]; g.N1 = pd->N[1]; g.N2 = pd->N[2];
   g.M = g.N0 / 2; g.Nh = g.M + 1; g.Nhp = (g.Nh + 1) & ~1; g.m = m;
@@ -119,13 +135,19 @@ extern "C" int rism3d_jacobian_apply_noalloc(const rism3d_problem *pd, int m, co
   g.dk0 = 2 * pi / pd->L[0]; g.dk1 = 2 * pi / pd->L[1]; g.dk2 = 2 * pi / pd->L[2];
   const double dkr = pi / pd->rmax;
   const double kmax = std::sqrt(std::pow(g.M * g.dk0, 2) + std::pow(g.N1 / 2 * g.dk1, 2) + std::pow(g.N2 / 2 * g.dk2, 2));
-  if ((int)(kmax / dkr) >= pd->nrad) return RISM3D_ERR_TABLE;
+  if ((int)(kmax / dkr) >= pd->nrad) {
+    set_last_error("rism3d_jacobian_apply_noalloc: |k| of the grid beyond the chi table");
+    return RISM3D_ERR_TABLE;
+  }
   // tile shapes of the FP64 runtime-length passes (8 complex per thread)
   int RX = 32, BY = 16, BZ = 16;
   while (RX > 1 && g.M * RX > 8 * 256) RX /= 2;
   while (BY > 4 && g.N1 * BY > 8 * 256) BY /= 2;
   while (BZ > 4 && g.N2 * BZ > 8 * 256) BZ /= 2;
-  if (g.N1 * BY > 8 * 256 || g.N2 * BZ > 8 * 256) return RISM3D_ERR_ARG;
+  if (g.N1 * BY > 8 * 256 || g.N2 * BZ > 8 * 256) {
+    set_last_error("rism3d_jacobian_apply_noalloc: grid too long along y or z");
+    return RISM3D_ERR_ARG;
+  }
   const int rows = g.N1 * g.N2;
   const int nblk = ((rows + RX - 1) / RX) * m;
   const int npair = m * (m + 1) / 2;
@@ -139,12 +161,13 @@ extern "C" int rism3d_jacobian_apply_noalloc(const rism3d_problem *pd, int m, co
   const size_t oCh = off;  off += up256(sizeof(double2) * (size_t)npair * pd->nrad);
   const size_t oPa = off;  off += up256(sizeof(NormPartial) * (size_t)nblk);
   if (off > kNoallocScratchBytes) {
-    g_msg = "grid needs " + std::to_string(off) + " bytes of scratch, the limit is " +
-            std::to_string(kNoallocScratchBytes);
+    set_last_error("rism3d_jacobian_apply_noalloc: the grid needs " + std::to_string(off) +
+                   " bytes of scratch, the limit is " + std::to_string(kNoallocScratchBytes));
     return RISM3D_ERR_ARG;
   }
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return RISM3D_ERR_CUDA;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail("cudaGetDevice", e);
   void *base = nullptr;
   int rc = setup(dev, &base);
   if (rc != RISM3D_OK) return rc;
@@ -153,13 +176,17 @@ extern "C" int rism3d_jacobian_apply_noalloc(const rism3d_problem *pd, int m, co
   // host-built tables copied in (no allocation on the device side)
   std::vector<double2> h;
   h.resize(g.M);  twiddles(g.M, h.data());
-  if (cudaMemcpy(S + oTx, h.data(), sizeof(double2) * g.M, cudaMemcpyHostToDevice) != cudaSuccess) return RISM3D_ERR_CUDA;
+  if ((e = cudaMemcpy(S + oTx, h.data(), sizeof(double2) * g.M, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cuda_fail("cudaMemcpy", e);
   h.resize(g.N1); twiddles(g.N1, h.data());
-  if (cudaMemcpy(S + oTy, h.data(), sizeof(double2) * g.N1, cudaMemcpyHostToDevice) != cudaSuccess) return RISM3D_ERR_CUDA;
+  if ((e = cudaMemcpy(S + oTy, h.data(), sizeof(double2) * g.N1, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cuda_fail("cudaMemcpy", e);
   h.resize(g.N2); twiddles(g.N2, h.data());
-  if (cudaMemcpy(S + oTz, h.data(), sizeof(double2) * g.N2, cudaMemcpyHostToDevice) != cudaSuccess) return RISM3D_ERR_CUDA;
+  if ((e = cudaMemcpy(S + oTz, h.data(), sizeof(double2) * g.N2, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cuda_fail("cudaMemcpy", e);
   h.resize(g.N0); twiddles(g.N0, h.data());
-  if (cudaMemcpy(S + oPo, h.data(), sizeof(double2) * g.Nh, cudaMemcpyHostToDevice) != cudaSuccess) return RISM3D_ERR_CUDA;
+  if ((e = cudaMemcpy(S + oPo, h.data(), sizeof(double2) * g.Nh, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cuda_fail("cudaMemcpy", e);
   // chi - delta as (value, slope) pairs, the interpolation of bgy3d-vec.c:22-46
   const int nrad = pd->nrad;
   std::vector<double2> tab((size_t)npair * nrad);
@@ -173,8 +200,8 @@ extern "C" int rism3d_jacobian_apply_noalloc(const rism3d_problem *pd, int m, co
         dst[k] = make_double2(row[k] - dl, ((row[ip] - dl) - (row[im] - dl)) / (ip - im));
       }
     }
-  if (cudaMemcpy(S + oCh, tab.data(), sizeof(double2) * tab.size(), cudaMemcpyHostToDevice) != cudaSuccess)
-    return RISM3D_ERR_CUDA;
+  if ((e = cudaMemcpy(S + oCh, tab.data(), sizeof(double2) * tab.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cuda_fail("cudaMemcpy", e);
   const AxisPlan px = plan_of(g.M, S + oTx), py = plan_of(g.N1, S + oTy), pz = plan_of(g.N2, S + oTz);
   const double2 *post = reinterpret_cast<const double2 *>(S + oPo);
   ZParams<double> zp{};
@@ -200,7 +227,9 @@ extern "C" int rism3d_jacobian_apply_noalloc(const rism3d_problem *pd, int m, co
   else k_y<double, true, 4><<<gy, 256, sy>>>(g, py, W);
   k_xinv<double><<<gx, 256, sx>>>(g, px, RX, W, dT, JdT, 1.0 / (double)g.Nr, 1.0, post,
                                   reinterpret_cast<NormPartial *>(S + oPa));
-  if (cudaGetLastError() != cudaSuccess) return RISM3D_ERR_CUDA;
-  if (cudaDeviceSynchronize() != cudaSuccess) return RISM3D_ERR_CUDA;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail("kernel launch", e);
+  // the calling thread's own default stream (the library is built with
+  // per-thread default streams): other threads' work is not waited for
+  if ((e = cudaStreamSynchronize(cudaStreamPerThread)) != cudaSuccess) return cuda_fail("cudaStreamSynchronize", e);
   return RISM3D_OK;
 }

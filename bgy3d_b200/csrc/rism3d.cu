@@ -1293,10 +1293,6 @@ NewtonOut newton(rism3d_ctx *c, TS *x, double tol, int max_iter, double krylov_r
   return o;
 }
 
-double now_s() {
-  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
-}
-
 int solve_impl(rism3d_ctx *c, double *T, rism3d_result *out) {
   rism3d_result res{};
   c->f_evals = c->jv_evals = c->f32_evals = c->jv32_evals = 0;
@@ -1674,6 +1670,41 @@ int response_impl(rism3d_ctx *c, const double *T, rism3d_grad *gr) {
       double a = 0.0;
       for (int b = 0; b < rb; ++b) a += hp[(size_t)q * rb + b];
       gr->dx[q] = a * f;
+    }
+  return RISM3D_OK;
+}
+
+// The reference's free-energy gradient at T (the `derivatives` output,
+// hnc3d.c:1665-1742): de[n][3] = rho h^3 sum_i <g_i, dv_i/dR_u> with the
+// field1 derivative, reduced on the device; any context (renormalised or
+// not, radial or 3D chi).  Host de, may be NULL (the sums are still made).
+int reference_gradient_impl(rism3d_ctx *c, const double *T, double *de) {
+  const rism3d_problem &pd = c->pd;
+  const Geo &G = c->g;
+  const int n = c->n;
+  if (c->pure) {
+    g_last_error = "the free-energy gradient needs a solute context";
+    return RISM3D_ERR_UNSUPPORTED;
+  }
+  if (n == 0) return RISM3D_OK;
+  constexpr int U = 4;
+  const double h0 = pd.L[0] / pd.N[0], h1 = pd.L[1] / pd.N[1], h2 = pd.L[2] / pd.N[2];
+  const int rb = (int)std::min<long long>(2 * 148, (G.Nr + 255) / 256);
+  double *part = dalloc<double>((size_t)rb * n * 3);
+  struct Free { double *p; ~Free() { dfree(p); } } fr{part};
+  k_force_pair<U><<<dim3(rb, (n + U - 1) / U), 256, 0, c->stream>>>(G, h0, h1, h2, pd.L[0], pd.L[1], pd.L[2],
+                                                                     c->d_solvent, n, c->d_solute, T, c->v64,
+                                                                     pd.beta, pd.closure, part);
+  CKL();
+  std::vector<double> hp((size_t)rb * n * 3);
+  CK(cudaMemcpyAsync(hp.data(), part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const double dN = pd.rho * c->h3;
+  for (int u = 0; u < n; ++u)
+    for (int d = 0; d < 3; ++d) {
+      double a = 0.0;
+      for (int q = 0; q < rb; ++q) a += hp[((size_t)u * rb + q) * 3 + d];
+      if (de) de[3 * u + d] = dN * a;
     }
   return RISM3D_OK;
 }
@@ -2728,18 +2759,29 @@ void d2h_large(void *dst, const void *src, size_t bytes, cudaStream_t st) {
     }
   }
   if (!sp.buf[0]) {
-    for (int b = 0; b < 2; ++b) CK(cudaHostAlloc(&sp.buf[b], kStageChunk, cudaHostAllocPortable));
+    CK(cudaHostAlloc(&sp.buf[0], kStageChunk, cudaHostAllocPortable));
+    const cudaError_t e = cudaHostAlloc(&sp.buf[1], kStageChunk, cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+      cudaFreeHost(sp.buf[0]);
+      g_last_error = std::string("cudaHostAlloc: ") + cudaGetErrorString(e);
+      throw CudaFail{RISM3D_ERR_NOMEM};
+    }
   }
+  // The pair goes back to the free list only once no copy into it can still
+  // be queued on st (an exception can leave the chunk loop with one in
+  // flight); if the stream cannot be drained the pair is dropped instead.
   struct Back {
     StagePair sp;
+    cudaStream_t st;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     ~Back() {
       for (auto e : ev)
         if (e) cudaEventDestroy(e);
+      if (cudaStreamSynchronize(st) != cudaSuccess) return;
       std::lock_guard<std::mutex> lk(g_stage_mu);
       g_stage_free.push_back(sp);
     }
-  } back{sp};
+  } back{sp, st};
   for (auto &e : back.ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   const unsigned hw = std::thread::hardware_concurrency();
   const int nthr = (int)std::max(1u, std::min(8u, hw ? hw : 1u));
@@ -2814,6 +2856,12 @@ template <typename F> int guard(F &&f) {
 }
 
 }  // namespace
+
+namespace rism {
+// Records the message that rism3d_last_error() returns on this thread (for
+// the library's other translation units).
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+}  // namespace rism
 
 // ================================================================== C ABI
 extern "C" {
@@ -3076,7 +3124,16 @@ int rism3d_jacobian_transpose_t1(rism3d_ctx *ctx, const double *T, const double 
 int rism3d_gradient(rism3d_ctx *ctx, const double *T, rism3d_grad *grad) {
   if (!ctx || !T || !grad) return RISM3D_ERR_ARG;
   if (ctx->pure) return RISM3D_ERR_UNSUPPORTED;
-  return guard([&] { return gradient_impl(ctx, T, grad); });
+  return guard([&] {
+    int rc = gradient_impl(ctx, T, grad);
+    if (rc == RISM3D_OK && grad->dx_reference) rc = reference_gradient_impl(ctx, T, grad->dx_reference);
+    return rc;
+  });
+}
+
+int rism3d_free_energy_gradient(rism3d_ctx *ctx, const double *T, double *de) {
+  if (!ctx || !T || !de) return RISM3D_ERR_ARG;
+  return guard([&] { return reference_gradient_impl(ctx, T, de); });
 }
 
 int rism3d_response(rism3d_ctx *ctx, const double *T, rism3d_grad *grad) {
@@ -3110,6 +3167,7 @@ int rism3d_solute_grad(const rism3d_problem *pd, int m, const rism3d_site *solve
     observables_impl(ctx, T, nullptr, &r);
     r.status = st;
     if (st == RISM3D_OK) st = gradient_impl(ctx, T, grad);
+    if (st == RISM3D_OK && grad->dx_reference) st = reference_gradient_impl(ctx, T, grad->dx_reference);
     if (t_inout) CK(cudaMemcpy(t_inout, T, bytes, cudaMemcpyDeviceToHost));
     if (out) *out = r;
     return st;

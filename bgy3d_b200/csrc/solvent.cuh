@@ -110,7 +110,7 @@ template <int MODE, int B, int MS>
 __global__ void __launch_bounds__(256) k_z_oz(Geo g, AxisPlan pz, double2 *__restrict__ W, PureParams<MS> pp) {
   using V = double2;
   constexpr int NP = MS * (MS + 1) / 2;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   V *tw = reinterpret_cast<V *>(smem_raw);
   V *buf = tw + pz.n;
   const int tid = threadIdx.x, nthr = blockDim.x;

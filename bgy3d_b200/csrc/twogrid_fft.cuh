@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(256) k_restrict_fx(long long rows, int Nc, int
   using Lay = LayRow<M, Split<M>::R2>;
   using Q = typename Quad<TI>::type;
   constexpr int N0 = 2 * M, PER = M / 2, CNT = (RX * PER + 255) / 256;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   V *tw = reinterpret_cast<V *>(smem_raw);
   V *buf = tw + M;
   V *C = buf + fx_buf<M, RX>();
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(256) k_prolong_fx(long long rows, int Nc, int 
   using Lay = LayRow<M, Split<M>::R2>;
   using QR = typename Quad<TR>::type;
   constexpr int N0 = 2 * M, H = M / 2 + 1, PER = M / 2, CNT = (RX * PER + 255) / 256;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   V *tw = reinterpret_cast<V *>(smem_raw);
   V *buf = tw + M;
   const int K1 = K + 1;
@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(256) k_restrict_fx2(long long rows, const TI *
   constexpr int N0 = 2 * M, Nc = 2 * MC, K = MC, K1 = MC + 1;
   constexpr int PER = M / 2, CNT = (RX * PER + 255) / 256;
   constexpr int PC = MC / 2;  // output float4 per row
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   V *tw = reinterpret_cast<V *>(smem_raw);
   V *buf = tw + M;
   V *X = buf + fx_buf<M, RX>();
@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(256, M == 128 ? 3 : 1) k_prolong_fx2(long long
   constexpr int N0 = 2 * M, Nc = 2 * MC, K = MC, K1 = MC + 1;
   constexpr int PER = M / 2, CNT = (RX * PER + 255) / 256;
   constexpr int YC = (RX * MC + 255) / 256;  // coarse pairs per thread
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   V *tw = reinterpret_cast<V *>(smem_raw);
   V *buf = tw + M;
   V *X = buf + fx_buf<M, RX>();

@@ -209,11 +209,14 @@ def hnc3d_run_solvent(solvent, settings, restart=None, want_g=True, want_restart
             "RESTART": t_out}
 
 
-def _grad_struct(n):
+def _grad_struct(n, reference=False):
     arrs = {k: np.zeros(n) for k in ("charge", "sigma", "epsilon")}
     arrs["x"] = np.zeros((n, 3))
     g = _abi.Grad()
     g.dq, g.dsigma, g.depsilon, g.dx = (_dptr(arrs[k]) for k in ("charge", "sigma", "epsilon", "x"))
+    if reference:
+        arrs["free-energy-gradient"] = np.zeros((n, 3))
+        g.dx_reference = _dptr(arrs["free-energy-gradient"])
     return g, arrs
 
 
@@ -225,7 +228,9 @@ def hnc3d_solute_grad(solute, solvent, settings, chi, restart=None):
     """Solve, then the free-energy gradient (rism3d_solute_grad): the result
     dict of hnc3d_run_solute (no GUV) with "gradient" = {"charge": dmu/dq
     [n], "sigma": [n], "epsilon": [n], "x": dmu/dx [n][3] (minus the
-    solvation force), "adjoint-jv", "adjoint-resid", "seconds"}."""
+    solvation force), "adjoint-jv", "adjoint-resid", "seconds"} and, as the
+    reference conses it with `derivatives` on, "free-energy-gradient"
+    [n][3] = rho h^3 sum_i <g_i, dv_i/dx_u> (hnc3d.c:1665-1742, 2289)."""
     L = _abi.lib()
     pd = problem_data(settings)
     m, n = len(solvent), len(solute)
@@ -237,12 +242,13 @@ def hnc3d_solute_grad(solute, solvent, settings, chi, restart=None):
     if t is not None and t.shape != shape:
         raise ValueError("restart has the wrong shape")
     res = _abi.Result()
-    g, arrs = _grad_struct(n)
+    g, arrs = _grad_struct(n, reference=True)
     rc = L.rism3d_solute_grad(ctypes.byref(pd), m, _sites(solvent), n, _sites(solute), _dptr(chi),
                               _dptr(t) if t is not None else None, ctypes.byref(res), ctypes.byref(g))
     if rc != _abi.OK:
         raise _abi.RismError(rc, "hnc3d_solute_grad")
     out = _result_dict(res)
+    out["free-energy-gradient"] = arrs.pop("free-energy-gradient")
     out["gradient"] = _grad_dict(g, arrs)
     out["RESTART"] = t
     return out
@@ -424,6 +430,14 @@ class RismContext:
         _abi.check(_abi.lib().rism3d_gradient(self._h, self._check_vec(T, self._torch.float64), ctypes.byref(g)),
                    "gradient")
         return _grad_dict(g, arrs)
+
+    def free_energy_gradient(self, T):
+        """The reference's "free-energy-gradient" [n][3] at a converged FP64 T:
+        rho h^3 sum_i <g_i, dv_i/dx_u> (rism3d_free_energy_gradient)."""
+        de = np.zeros((self.n, 3))
+        _abi.check(_abi.lib().rism3d_free_energy_gradient(self._h, self._check_vec(T, self._torch.float64),
+                                                          _dptr(de)), "free_energy_gradient")
+        return de
 
     def response(self, T):
         """Linear-response dmu/dx [n][3] at a converged FP64 T (rism3d_response,

@@ -86,7 +86,7 @@ typedef struct rism3d_problem {
   /* Krylov solver of the Newton steps.  krylov_restart 30, ew_forcing 0 and
      coarse_h 0 are the reference's settings: GMRES(30) without
      preconditioner at a fixed KSP rtol of 1e-3 (bgy3d-snes.c:262-306).
-     rism3d_problem_defaults() selects 30 / 1 / 0.75 / 12. */
+     rism3d_problem_defaults() selects 30 / 1 / 0.75 / 16. */
   int krylov_restart; /* GMRES restart length (0: 30) */
   int ew_forcing;     /* 1: Eisenstat-Walker forcing terms, floored at 1e-3;
                          0: fixed rtol 1e-3 */
@@ -154,6 +154,9 @@ typedef struct rism3d_grad {
   int adjoint_jv;     /* J.v products of the adjoint solve */
   double adjoint_resid; /* ||J^T lambda - dmu/dt||_2 / ||dmu/dt||_2 */
   double seconds;     /* device time of the gradient */
+  double *dx_reference; /* [n][3] or NULL: the reference's own
+                         free-energy-gradient, rho h^3 sum_i <g_i, dv_i/dx_u>
+                         (see rism3d_free_energy_gradient) */
 } rism3d_grad;
 
 /*
@@ -165,7 +168,8 @@ typedef struct rism3d_grad {
   dmu/dp = d mu/dp|_t - lambda . dF/dp|_t, exact for any closure's
   functional and for the renormalised long-range term.  Arguments as
   rism3d_solute_solve (t_inout may be NULL).  Renormalised form only
-  (RISM3D_ERR_UNSUPPORTED with renorm = 0).
+  (RISM3D_ERR_UNSUPPORTED with renorm = 0).  With grad->dx_reference set it
+  also receives the reference's own formula (rism3d_free_energy_gradient).
 */
 int rism3d_solute_grad(const rism3d_problem *pd,
                        int m, const rism3d_site *solvent,
@@ -275,6 +279,19 @@ int rism3d_jacobian_transpose_t1(rism3d_ctx *ctx, const double *T, const double 
    rism3d_solute_grad. */
 int rism3d_gradient(rism3d_ctx *ctx, const double *T, rism3d_grad *grad);
 
+/* The `derivatives` output of hnc3d_solute_solve, consed as
+   "free-energy-gradient" (gradients / energy1, hnc3d.c:1665-1742, 2270-2289):
+   de[u][a] = rho h^3 sum_i sum_r g_i(r) dv_i(r)/dx_{u,a}, g = c(T) + T + 1
+   and dv the derivative of the solute field for a unit displacement of site
+   u (field1, bgy3d-solutes.c:381-468: LJ and the FULL capped Coulomb; 0 at
+   a grid point on the site).  The formula takes mu as stationary in t and
+   the Coulomb derivative in real space; rism3d_gradient differentiates the
+   renormalised, periodic functional exactly, and the two differ by about
+   1 % of the largest component (0.8-0.9 % on the test solutes).  T:
+   converged FP64 device pointer; de: host [n][3].  Any solute context
+   (renormalised or not, radial or 3D chi). */
+int rism3d_free_energy_gradient(rism3d_ctx *ctx, const double *T, double *de);
+
 /* Linear-response derivatives dmu/dx_u[n][3] at a converged T (FP64
    device pointer), as the `response` branch of hnc3d_solute_solve computes
    them ("free-energy-response", hnc3d.c:1969-2135 with response_t1,
@@ -322,10 +339,14 @@ int rism3d_profile(rism3d_ctx *ctx, int on, double *ms, long long *launches);
    32 MiB file-scope device array held by every device that loads the
    library until exit; grids whose scratch exceeds it return RISM3D_ERR_ARG
    (m = 3 fits up to 96^3).  chi is the host [m][m][nrad] table as for
-   rism3d_ctx_create; dT, JdT are device pointers; default stream, returns
-   after the result is complete.  The first call on a device looks up the
-   array's device address (make it before any stream capture).  All calls
-   share the array: calls that overlap on the GPU race. */
+   rism3d_ctx_create; d, dT, JdT are device pointers.  The work runs on the
+   calling host thread's per-thread default stream (cudaStreamPerThread; the
+   library is built with per-thread default streams), so d and dT must be
+   complete with respect to that stream; the call returns after the result
+   is complete, without waiting for other streams.  The first call on a
+   device looks up the array's device address (make it before any stream
+   capture).  All calls share the array: calls that overlap on the GPU
+   race.  Failures leave a message for rism3d_last_error(). */
 int rism3d_jacobian_apply_noalloc(const rism3d_problem *pd, int m, const double *chi,
                                   const double *d, const double *dT, double *JdT);
 

@@ -7,6 +7,8 @@ DMDA order of bgy3d-fftw3.c:295-339); k-fields are [N2][N1][N0/2+1]
 (FFTW r2c halving the stride-1 dimension, bgy3d-fftw3.c:374-385).
 FFTW's unnormalised r2c/c2r map onto scipy.fft rfftn / (N * irfftn).
 """
+from concurrent.futures import ThreadPoolExecutor
+
 import numpy as np
 import scipy.fft
 import scipy.special
@@ -111,19 +113,21 @@ def kfreq(i, n):
     return np.where(i <= n // 2, i, i - n)
 
 
-def rgrid(N, L):
-    """vec_rmap3 (bgy3d-vec.h:578-607): r = i h - L/2, arrays [z][y][x]."""
+def rgrid(N, L, zs=slice(None)):
+    """vec_rmap3 (bgy3d-vec.h:578-607): r = i h - L/2, arrays [z][y][x]
+    (the z planes ``zs`` only)."""
     h = [L[d] / N[d] for d in range(3)]
     ax = [np.arange(N[d]) * h[d] - L[d] / 2 for d in range(3)]
-    return ax[0][None, None, :], ax[1][None, :, None], ax[2][:, None, None]
+    return ax[0][None, None, :], ax[1][None, :, None], ax[2][zs][:, None, None]
 
 
-def kgrid(N, L):
-    """vec_kmap3 (bgy3d-vec.h:613-648): k = KFREQ(i) * 2 pi / L on [N2][N1][N0/2+1]."""
+def kgrid(N, L, zs=slice(None)):
+    """vec_kmap3 (bgy3d-vec.h:613-648): k = KFREQ(i) * 2 pi / L on [N2][N1][N0/2+1]
+    (the kz planes ``zs`` only)."""
     dk = [2 * np.pi / L[d] for d in range(3)]
     i0 = np.arange(N[0] // 2 + 1)
     i1 = np.arange(N[1])
-    i2 = np.arange(N[2])
+    i2 = np.arange(N[2])[zs]
     k0 = (kfreq(i0, N[0]) * dk[0])[None, None, :]
     k1 = (kfreq(i1, N[1]) * dk[1])[None, :, None]
     k2 = (kfreq(i2, N[2]) * dk[2])[:, None, None]
@@ -133,8 +137,8 @@ def kgrid(N, L):
     return k0, k1, k2, sign
 
 
-def kabs(N, L):
-    k0, k1, k2, _ = kgrid(N, L)
+def kabs(N, L, zs=slice(None)):
+    k0, k1, k2, _ = kgrid(N, L, zs)
     return np.sqrt((k0 ** 2 + k1 ** 2) + k2 ** 2)
 
 
@@ -152,13 +156,13 @@ def interp(x, xtab, dx):
 
 
 # ------------------------------------------------------------- setup
-def solute_field(N, L, solvent, solute):
-    """field0 (bgy3d-solutes.c:343-377): v[m][N2][N1][N0]."""
-    x, y, z = rgrid(N, L)
+def solute_field(N, L, solvent, solute, zs=slice(None)):
+    """field0 (bgy3d-solutes.c:343-377): v[m][N2][N1][N0] (z planes ``zs``)."""
+    x, y, z = rgrid(N, L, zs)
     m = len(solvent)
-    v = np.zeros((m, N[2], N[1], N[0]))
+    v = np.zeros((m, z.shape[0], N[1], N[0]))
     for i, a in enumerate(solvent):
-        e = np.zeros((N[2], N[1], N[0]))
+        e = np.zeros((z.shape[0], N[1], N[0]))
         for b in solute:
             eab = np.sqrt(a["epsilon"] * b["epsilon"])
             sab = 0.5 * (a["sigma"] + b["sigma"])
@@ -197,10 +201,11 @@ def coulomb_long(N, L, solute):
     return EPSILON0INV * s
 
 
-def form_factor_centered(N, L, solute):
-    """solute_form (bgy3d-solutes.c:633-660): sum q e^{-ik.x} times (-1)^(ix+iy+iz)."""
-    k0, k1, k2, sign = kgrid(N, L)
-    f = np.zeros((N[2], N[1], N[0] // 2 + 1), dtype=np.complex128)
+def form_factor_centered(N, L, solute, zs=slice(None)):
+    """solute_form (bgy3d-solutes.c:633-660): sum q e^{-ik.x} times (-1)^(ix+iy+iz)
+    (kz planes ``zs``)."""
+    k0, k1, k2, sign = kgrid(N, L, zs)
+    f = np.zeros((k2.shape[0], N[1], N[0] // 2 + 1), dtype=np.complex128)
     for b in solute:
         bx = b["x"]
         f = f + b["charge"] * np.exp(-1j * ((k0 * bx[0] + k1 * bx[1]) + k2 * bx[2]))
@@ -224,9 +229,14 @@ def renorm_kernel(solvent, chi, rmax, alpha=G):
 
 
 class Problem:
-    """Everything hnc3d_solute_solve sets up before SNES (hnc3d.c:1790-1966)."""
+    """Everything hnc3d_solute_solve sets up before SNES (hnc3d.c:1790-1966).
 
-    def __init__(self, N, L, beta, rho, closure, solvent, solute, chi, rmax, renorm=True, chi3=None):
+    ``threads`` > 1 evaluates the pointwise work (setup, closure, OZ
+    contraction, scaling) on z-slabs in a thread pool and the FFTs with
+    that many workers: the same arithmetic per grid point, for timing the
+    restatement on every host core."""
+
+    def __init__(self, N, L, beta, rho, closure, solvent, solute, chi, rmax, renorm=True, chi3=None, threads=1):
         """chi: [m][m][nrad] radial chi table, or None with chi3 = chi - 1 on
         the k grid (packed pairs [m(m+1)/2][N2][N1][N0/2+1], complex), the
         --solvent-3d kernel read from x%d%d-fft.bin (solvent_kernel_file,
@@ -240,55 +250,91 @@ class Problem:
         self.renorm = renorm
         self.h3 = self.h[0] * self.h[1] * self.h[2]
         self.L3 = self.L[0] * self.L[1] * self.L[2]
-        kk = kabs(self.N, self.L)
+        self.threads = max(1, int(threads))
+        self.workers = self.threads if self.threads > 1 else _WORKERS
+        self._pool = ThreadPoolExecutor(self.threads) if self.threads > 1 else None
         m = self.m
+        nk = (self.N[2], self.N[1], self.N[0] // 2 + 1)
         if chi3 is not None:
             renorm = self.renorm = False
-            self.chi_fft = np.zeros((m, m) + kk.shape, dtype=complex)
+            self.chi_fft = np.zeros((m, m) + nk, dtype=complex)
             p = 0
             for i in range(m):
                 for j in range(i + 1):
                     self.chi_fft[i, j] = self.chi_fft[j, i] = chi3[p]
                     p += 1
         else:
-            nrad = chi.shape[-1]
             dk = np.pi / rmax
-            self.chi_fft = np.zeros((m, m) + kk.shape)
-            for i in range(m):
-                for j in range(i + 1):
-                    tab = chi[i, j] - (1.0 if i == j else 0.0)
-                    self.chi_fft[i, j] = interp(kk, tab, dk)
-                    self.chi_fft[j, i] = self.chi_fft[i, j]
+            self.chi_fft = np.zeros((m, m) + nk)
         self.charge = np.array([s["charge"] for s in solvent])
-        F = form_factor_centered(self.N, self.L, solute)
         if renorm:
-            s = renorm_kernel(solvent, chi, rmax)
-            self.tau_fft = np.stack([interp(kk, s[i], dk) * F for i in range(m)])
+            srad = renorm_kernel(solvent, chi, rmax)
+            self.tau_fft = np.zeros((m,) + nk, dtype=complex)
             self.v_long_fft = None
         else:
             self.tau_fft = None
-            # bgy3d-force.h:139-148 coulomb_long_fourier(k, q2=1, G), corner;
-            # centred through F (bgy3d-solutes.c:766-792)
-            self.v_long_fft = EPSILON0INV * coulomb_long_fourier(kk, G) * F
-        self.v = solute_field(self.N, self.L, solvent, solute)
+            self.v_long_fft = np.zeros(nk, dtype=complex)
+        self.v = np.zeros((m, self.N[2], self.N[1], self.N[0]))
+
+        def setup(a, b):
+            zs = slice(a, b)
+            kk = kabs(self.N, self.L, zs)
+            if chi3 is None:
+                for i in range(m):
+                    for j in range(i + 1):
+                        tab = chi[i, j] - (1.0 if i == j else 0.0)
+                        self.chi_fft[i, j, a:b] = interp(kk, tab, dk)
+                        self.chi_fft[j, i, a:b] = self.chi_fft[i, j, a:b]
+            F = form_factor_centered(self.N, self.L, solute, zs)
+            if renorm:
+                for i in range(m):
+                    self.tau_fft[i, a:b] = interp(kk, srad[i], dk) * F
+            else:
+                # bgy3d-force.h:139-148 coulomb_long_fourier(k, q2=1, G), corner;
+                # centred through F (bgy3d-solutes.c:766-792)
+                self.v_long_fft[a:b] = EPSILON0INV * coulomb_long_fourier(kk, G) * F
+            self.v[:, a:b] = solute_field(self.N, self.L, solvent, solute, zs)
+
+        self._each_slab(setup)
+
+    def _each_slab(self, fn):
+        """fn(a, b) over z-slabs [a, b) of the grid (k grids: kz planes)."""
+        n2 = self.N[2]
+        if self._pool is None:
+            fn(0, n2)
+            return
+        k = min(n2, 4 * self.threads)
+        cuts = [n2 * q // k for q in range(k + 1)]
+        for f in [self._pool.submit(fn, cuts[q], cuts[q + 1]) for q in range(k) if cuts[q] < cuts[q + 1]]:
+            f.result()
 
     # -- FFT MatShell (bgy3d-fftw3.c:229-265), unnormalised ------------
     def fft(self, x):
-        return scipy.fft.rfftn(x, axes=(-3, -2, -1), workers=_WORKERS)
+        return scipy.fft.rfftn(x, axes=(-3, -2, -1), workers=self.workers)
 
     def ifft(self, y):
         n = self.N[0] * self.N[1] * self.N[2]
         return scipy.fft.irfftn(y, s=(self.N[2], self.N[1], self.N[0]), axes=(-3, -2, -1),
-                                workers=_WORKERS) * n
+                                workers=self.workers) * n
 
     def star(self, c_fft):
         """hnc3d.c:1114-1138."""
         return np.einsum("ijk...,jk...->ik...", self.chi_fft.reshape(self.m, self.m, -1),
                          c_fft.reshape(self.m, -1)).reshape(c_fft.shape)
 
+    def _star_slab(self, cf, a, b):
+        """star on the kz planes [a, b): t_i = sum_j (chi-1)_ij c_j."""
+        out = np.zeros_like(cf)
+        for i in range(self.m):
+            for j in range(self.m):
+                out[i] += self.chi_fft[i, j, a:b] * cf[j]
+        return out
+
     def iterate_t1(self, T):
         """hnc3d.c:1183-1285: dT = (chi-1)*c(t) [- beta/eps0 tau] - t."""
         beta = self.beta
+        if self._pool is not None:
+            return self._iterate_t1_slabs(T)
         c = cl.closure(self.closure, beta, self.v, T)
         c_fft = self.fft(c) * self.h3
         if not self.renorm:
@@ -300,8 +346,62 @@ class Problem:
             t_fft = t_fft - (beta * self.charge)[:, None, None, None] * self.v_long_fft
         return self.ifft(t_fft) * (1.0 / self.L3) - T
 
+    def _iterate_t1_slabs(self, T):
+        beta = self.beta
+        c = np.empty_like(T)
+
+        def clo(a, b):
+            c[:, a:b] = cl.closure(self.closure, beta, self.v[:, a:b], T[:, a:b])
+
+        self._each_slab(clo)
+        c_fft = self.fft(c)
+        t_fft = np.empty_like(c_fft)
+
+        def oz(a, b):
+            cf = c_fft[:, a:b] * self.h3
+            if not self.renorm:
+                cf = cf - (beta * self.charge)[:, None, None, None] * self.v_long_fft[a:b]
+            tf = self._star_slab(cf, a, b)
+            if self.renorm:
+                tf -= (beta * EPSILON0INV) * self.tau_fft[:, a:b]
+            else:
+                tf -= (beta * self.charge)[:, None, None, None] * self.v_long_fft[a:b]
+            t_fft[:, a:b] = tf
+
+        self._each_slab(oz)
+        r = self.ifft(t_fft)
+
+        def fin(a, b):
+            r[:, a:b] *= 1.0 / self.L3
+            r[:, a:b] -= T[:, a:b]
+
+        self._each_slab(fin)
+        return r
+
     def jacobian_t1(self, T, dT):
         """hnc3d.c:1289-1362: J dT = (chi-1)*(c'(t) dT) - dT."""
+        if self._pool is not None:
+            dc = np.empty_like(T)
+
+            def clo(a, b):
+                dc[:, a:b] = cl.closure1(self.closure, self.beta, self.v[:, a:b], T[:, a:b], dT[:, a:b])
+
+            self._each_slab(clo)
+            c_fft = self.fft(dc)
+            t_fft = np.empty_like(c_fft)
+
+            def oz(a, b):
+                t_fft[:, a:b] = self._star_slab(c_fft[:, a:b] * self.h3, a, b)
+
+            self._each_slab(oz)
+            r = self.ifft(t_fft)
+
+            def fin(a, b):
+                r[:, a:b] *= 1.0 / self.L3
+                r[:, a:b] -= dT[:, a:b]
+
+            self._each_slab(fin)
+            return r
         dc = cl.closure1(self.closure, self.beta, self.v, T, dT)
         t_fft = self.star(self.fft(dc) * self.h3)
         return self.ifft(t_fft) * (1.0 / self.L3) - dT

@@ -8,6 +8,8 @@ Checks, in FP64:
     |F|inf < 1e-13: agreement to 2e-5 (absolute, kcal/mol per unit) plus
     2e-5 relative;
   * the torch.autograd.Function reproduces the API gradient;
+  * the reference's own "free-energy-gradient" output (rism3d_free_energy_
+    gradient) against the oracle's restatement to 1e-10 relative;
   * dmu/dx against the reference's own solute forces, rho h^3 sum_i
     <g_i, dv_i/dx> with the full capped Coulomb (hnc3d.c:1665-1742,
     bgy3d-solutes.c:381-468, restated by oracle.hnc3d.solute_field1).  That
@@ -132,3 +134,30 @@ def test_forces_close_to_reference_formula(fixture_loader, name):
     err = np.max(np.abs(got - ref)) / np.max(np.abs(ref))
     print(f"{name}: adjoint vs reference-formula forces, max deviation {err:.3e} of max |F|")
     assert err < 0.02
+
+
+@pytest.mark.parametrize("name", CASES + ["na_kh_n32", "water_hnc_norenorm_n24"])
+def test_reference_free_energy_gradient(fixture_loader, name):
+    """The reference's own `derivatives` output ("free-energy-gradient",
+    hnc3d.c:1665-1742): rho h^3 sum_i <g_i, dv_i/dx_u> reduced on the device
+    (rism3d_free_energy_gradient) against the oracle's restatement of the
+    same sum at the same converged t, to 1e-10 of the largest component;
+    the charged and the no-renorm cases included.  hnc3d_solute_grad returns
+    the same array beside the adjoint gradient."""
+    meta, arr = fixture_loader(name)
+    s = meta["settings"]
+    ctx = RismContext(meta["solute"], meta["solvent"], settings_of(meta), arr["chi"])
+    got = ctx.free_energy_gradient(to_dev(arr["T"]))
+    ctx.close()
+    P = problem(meta, arr)
+    g = P.observables(arr["T"])["g"]
+    N = (s["N"],) * 3
+    L = (2 * s["L"],) * 3
+    ref = np.array([[s["rho"] * P.h3 * np.sum(g * hnc3d.solute_field1(N, L, meta["solvent"], meta["solute"], u, d))
+                     for d in range(3)] for u in range(len(meta["solute"]))])
+    scale = np.max(np.abs(ref))
+    assert np.max(np.abs(got - ref)) < 1e-10 * scale
+    if not s["no-renorm"]:
+        res = hnc3d_solute_grad(meta["solute"], meta["solvent"], settings_of(meta, **{"norm-tol": 1e-12}),
+                                arr["chi"], restart=arr["T"])
+        assert np.max(np.abs(res["free-energy-gradient"] - ref)) < 1e-8 * scale

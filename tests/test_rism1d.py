@@ -15,6 +15,8 @@ WATER = find_molecule("water, PR-SPC/E")
     (40.0, 1536, cl.HNC, 78.4),    # the grid hnc3d_solute_solve upscales to
     (32.0, 512, cl.KH, 78.4),
     (20.0, 256, cl.HNC, 0.0),      # plain RISM, no dielectric correction
+    (160.0, 4096, cl.HNC, 78.4),   # the grid every benchmark configuration uses (README:16 solvent)
+    (160.0, 4096, cl.KH, 78.4),    # the chi of the benched 256^3 KH workload
 ])
 def test_chi_matches_oracle(rmax, nrad, closure, eps):
     s = {"rmax": rmax, "nrad": nrad, "rho": 0.0333295, "beta": 1.6889, "dielectric": eps,
