@@ -95,18 +95,20 @@ template <int N, int R2> struct LayRow {
   __device__ __forceinline__ static int at(int i, int row) { return row * RS + i + i / R2; }
 };
 
-// Two-step transform of NCOL columns of length N.  COLFAST maps consecutive
-// threads to consecutive columns (column-contiguous tiles), otherwise to
-// consecutive transform indices (row-contiguous tiles).  Ends synchronised.
+// Two-step transform of NCOL columns of length N by NTHR threads (tid <
+// NTHR; threads with act false only take part in the barriers, so several
+// groups of one CTA can transform their own tiles together).  COLFAST maps
+// consecutive threads to consecutive columns (column-contiguous tiles),
+// otherwise to consecutive transform indices (row-contiguous tiles).  Ends
+// synchronised.
 template <int N, int NCOL, int NTHR, bool INV, bool COLFAST, class Lay, typename V>
-__device__ __forceinline__ void fft2(V *buf, const V *tw) {
+__device__ __forceinline__ void fft2g(V *buf, const V *tw, int tid, bool act) {
   constexpr int R1 = Split<N>::R1, R2 = Split<N>::R2;
-  const int tid = threadIdx.x;
   constexpr int I1 = R2 * NCOL;
 #pragma unroll
   for (int it = 0; it < (I1 + NTHR - 1) / NTHR; ++it) {
     const int w = tid + it * NTHR;
-    if (I1 % NTHR == 0 || w < I1) {
+    if (act && (I1 % NTHR == 0 || w < I1)) {
       const int col = COLFAST ? w % NCOL : w / R2;
       const int n2 = COLFAST ? w / NCOL : w % R2;
       V u[R1];
@@ -132,7 +134,7 @@ __device__ __forceinline__ void fft2(V *buf, const V *tw) {
 #pragma unroll
   for (int it = 0; it < C2; ++it) {
     const int w = tid + it * NTHR;
-    if (I2 % NTHR == 0 || w < I2) {
+    if (act && (I2 % NTHR == 0 || w < I2)) {
       const int col = COLFAST ? w % NCOL : w / R1;
       const int k1 = COLFAST ? w / NCOL : w % R1;
 #pragma unroll
@@ -144,7 +146,7 @@ __device__ __forceinline__ void fft2(V *buf, const V *tw) {
 #pragma unroll
   for (int it = 0; it < C2; ++it) {
     const int w = tid + it * NTHR;
-    if (I2 % NTHR == 0 || w < I2) {
+    if (act && (I2 % NTHR == 0 || w < I2)) {
       const int col = COLFAST ? w % NCOL : w / R1;
       const int k1 = COLFAST ? w / NCOL : w % R1;
 #pragma unroll
@@ -152,6 +154,11 @@ __device__ __forceinline__ void fft2(V *buf, const V *tw) {
     }
   }
   __syncthreads();
+}
+// The whole CTA as one group of NTHR threads.
+template <int N, int NCOL, int NTHR, bool INV, bool COLFAST, class Lay, typename V>
+__device__ __forceinline__ void fft2(V *buf, const V *tw) {
+  fft2g<N, NCOL, NTHR, INV, COLFAST, Lay>(buf, tw, (int)threadIdx.x, true);
 }
 
 // ------------------------------------------------------------- TMA + mbarrier

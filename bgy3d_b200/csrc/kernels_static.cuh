@@ -275,16 +275,20 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_y_s(Geo g, const __grid_co
 // One z tile in shared memory: forward transform along z of the m [N][B]
 // site columns, the OZ contraction with the radial chi-1 tables (+ the
 // long-range terms in MODE_F), inverse transform; ends after a barrier.
-template <typename T, int MODE, int N, int B, int MS>
-__device__ __forceinline__ void z_tile(const Geo &g, typename Cx<T>::type *buf, const typename Cx<T>::type *tw,
-                                       const ZParams<T> &zp, int kx0, int y) {
+// Run by the NTHR = R1 B threads tid of a group (act false: barriers only);
+// JOINT: the MS site tiles (all allocated) transform as one MS B-column
+// tile by R1 B MS threads.
+template <typename T, int MODE, int N, int B, int MS, bool JOINT = false>
+__device__ __forceinline__ void z_tile_g(const Geo &g, typename Cx<T>::type *buf, const typename Cx<T>::type *tw,
+                                         const ZParams<T> &zp, int kx0, int y, int tid, bool act) {
   using V = typename Cx<T>::type;
   using P2 = typename Vec2<T>::type;
-  constexpr int NTHR = Split<N>::R1 * B;
+  constexpr int NTHR = Split<N>::R1 * B * (JOINT ? MS : 1);
   const int m = g.m;
-  const int tid = threadIdx.x;
   const int bw = min(B, g.Nh - kx0);
-  for (int s = 0; s < m; ++s) fft2<N, B, NTHR, false, true, LayCol<N, B>>(buf + s * N * B, tw);
+  if (JOINT) fft2g<N, MS * B, NTHR, false, true, LayCol<N, B>>(buf, tw, tid, act);
+  else
+    for (int s = 0; s < m; ++s) fft2g<N, B, NTHR, false, true, LayCol<N, B>>(buf + s * N * B, tw, tid, act);
   const int ky = kfreq(y, g.N1);
   const double k1 = ky * g.dk1;
   const long long zstride = (long long)g.N1 * g.Nhp;
@@ -295,7 +299,7 @@ __device__ __forceinline__ void z_tile(const Geo &g, typename Cx<T>::type *buf, 
   const int np = m * (m + 1) / 2;
   const bool full = MODE == MODE_F && zp.L != nullptr;
 #pragma unroll 2
-  for (int e = tid; e < N * B; e += NTHR) {
+  for (int e = act ? tid : N * B; e < N * B; e += NTHR) {
     const int z = e / B, b = e % B;
     const bool valid = b < bw;
     const int kx = kx0 + b;
@@ -358,7 +362,14 @@ __device__ __forceinline__ void z_tile(const Geo &g, typename Cx<T>::type *buf, 
     }
   }
   __syncthreads();
-  for (int s = 0; s < m; ++s) fft2<N, B, NTHR, true, true, LayCol<N, B>>(buf + s * N * B, tw);
+  if (JOINT) fft2g<N, MS * B, NTHR, true, true, LayCol<N, B>>(buf, tw, tid, act);
+  else
+    for (int s = 0; s < m; ++s) fft2g<N, B, NTHR, true, true, LayCol<N, B>>(buf + s * N * B, tw, tid, act);
+}
+template <typename T, int MODE, int N, int B, int MS>
+__device__ __forceinline__ void z_tile(const Geo &g, typename Cx<T>::type *buf, const typename Cx<T>::type *tw,
+                                       const ZParams<T> &zp, int kx0, int y) {
+  z_tile_g<T, MODE, N, B, MS>(g, buf, tw, zp, kx0, y, (int)threadIdx.x, true);
 }
 
 // z pass: the m [N][B] tiles of one (ky, kx-block) by TMA, forward transform,

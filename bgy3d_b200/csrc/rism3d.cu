@@ -26,6 +26,7 @@
 #include <tuple>
 #include <vector>
 
+#include "coarse_pk.cuh"
 #include "kernels.cuh"
 #include "kernels_static.cuh"
 #include "grad.cuh"
@@ -40,6 +41,9 @@ using namespace rism;
 
 namespace rism {  // twogrid_fx2.cu: x transfers with both sides by FFT
 bool fx2_has_pair(int M, int MC);
+// coarse_pk.cu: the persistent cooperative coarse GMRES
+int coarse_pk_grid(int M, int N, int per_sm);
+cudaError_t coarse_pk_launch(const PkArgs &a, int M, int N, int grid, cudaStream_t st);
 template <typename T>
 bool fx2_restrict(int M, int MC, long long rows, const T *in, float s, const float2 *post, const float2 *tw,
                   const float2 *postc, const float2 *twc, float *out, cudaStream_t st);
@@ -257,6 +261,13 @@ struct rism3d_ctx {
   unsigned *cg_ticket = nullptr;              // last-block ticket of the fused sweeps
   long long cg_nodes = 0;
   bool cg_failed = false;
+  // the coarse solve as one persistent cooperative kernel (coarse_pk.cuh)
+  double *pk_dot = nullptr, *pk_nrm = nullptr;  // block partials of its reductions
+  unsigned *pk_bar = nullptr;                   // its grid-barrier counter
+  int pk_grid = 0;                              // CTAs (0: not set up)
+  bool pk_failed = false;                       // shape or device without it
+  int coarse_driver = -1;  // of the last coarse solve: 0 host-driven, 1 graph, 2 persistent kernel
+  unsigned long long *pk_trace = nullptr;       // RISM3D_PK_TRACE: phase timestamps
 
   cudaStream_t stream = 0;
   PassTimer timer;
@@ -283,6 +294,7 @@ struct rism3d_ctx {
     for (auto p : zbasis32) fr(p);
     for (int a = 0; a < 3; ++a) { fr(tR[a]); fr(tRt[a]); fr(tP[a]); fr(tPt[a]); }
     fr(tA); fr(tB); fr(tc_r); fr(tc_y); fr(cg_H); fr(cg_aux); fr(cg_ticket); fr(tC); fr(tD);
+    fr(pk_dot); fr(pk_nrm); fr(pk_bar); fr(pk_trace);
     if (cg_exec) cudaGraphExecDestroy(cg_exec);
     if (cg_graph) cudaGraphDestroy(cg_graph);
     delete coarse;
@@ -559,7 +571,8 @@ void reduce_norms(rism3d_ctx *c, int nblk, double *resid) {
   CK(cudaMemcpyAsync(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (err) {
-    g_last_error = "a bounded TMA/mbarrier wait timed out in pass " + std::to_string(err);
+    g_last_error = err == kPkErr ? std::string("a bounded grid-barrier wait timed out in the coarse solve")
+                                 : "a bounded TMA/mbarrier wait timed out in pass " + std::to_string(err);
     throw CudaFail{RISM3D_ERR_CUDA};
   }
   double amax = 0.0, s2 = 0.0;
@@ -1094,16 +1107,130 @@ bool coarse_graph(rism3d_ctx *c, int k) {
   return ok;
 }
 
+// Solves issued by concurrent host threads (the batch driver) keep the
+// graph-replayed coarse solve: cooperative grids of several streams could
+// each hold part of the GPU while waiting for the rest.
+thread_local bool tl_concurrent_solves = false;
+
+// The persistent coarse GMRES is used when the coarse grid is a cube with
+// shape-specialised transforms, m <= 3 and k <= 16 (RISM3D_COARSE_PERSIST=0
+// turns it off); its buffers are allocated on first use.
+bool coarse_pk_ready(rism3d_ctx *c, int k) {
+  if (c->pk_grid > 0) return !tl_concurrent_solves;
+  if (c->pk_failed || tl_concurrent_solves) return false;
+  const char *env = std::getenv("RISM3D_COARSE_PERSIST");
+  rism3d_ctx *cc = c->coarse;
+  const Geo &G = cc->g;
+  if ((env && env[0] == '0') || !cc->stat[1] || cc->pure || G.m > 3 || k < 1 || k > kPkMaxSteps ||
+      G.N0 != G.N1 || G.N1 != G.N2) {
+    c->pk_failed = true;
+    return false;
+  }
+  const char *per = std::getenv("RISM3D_PK_CTAS_PER_SM");  // CTAs per SM (default 2)
+  const int grid = coarse_pk_grid(G.M, G.N1, per ? std::atoi(per) : 2);
+  if (grid <= 0) {
+    c->pk_failed = true;
+    cudaGetLastError();
+    return false;
+  }
+  ensure_basis<float>(cc, k + 1);
+  slopebuf<float>(cc);
+  c->pk_dot = dalloc<double>((size_t)grid * kVecMax);
+  c->pk_nrm = dalloc<double>((size_t)2 * grid);
+  c->pk_bar = dalloc<unsigned>(1);
+  if (!c->cg_H) c->cg_H = dalloc<double>((size_t)k * (k + 1));
+  if (!c->cg_aux) c->cg_aux = dalloc<double>((size_t)k + 2);
+  c->pk_grid = grid;
+  return true;
+}
+
+// J_H^-1 r + r into tc_y by the persistent kernel, r in coarse basis slot 0.
+// False (and the kernel off for this context) if the launch is refused.
+bool coarse_pk_run(rism3d_ctx *c, int k) {
+  rism3d_ctx *cc = c->coarse;
+  auto &B = basis<float>(cc);
+  PkArgs a{};
+  a.g = cc->g;
+  a.W = cc->work<float>();
+  for (int i = 0; i <= k; ++i) a.V[i] = B[i];
+  a.d = slopebuf<float>(cc);
+  a.out = c->tc_y;
+  a.post = postw<float>(cc);
+  a.twx = static_cast<const float2 *>(cc->plan<float>(0).tw);
+  a.twy = static_cast<const float2 *>(cc->plan<float>(1).tw);
+  a.twz = static_cast<const float2 *>(cc->plan<float>(2).tw);
+  a.zp = zparams<float>(cc, false);
+  a.pdot = c->pk_dot;
+  a.pnrm = c->pk_nrm;
+  a.H = c->cg_H;
+  a.aux = c->cg_aux;
+  a.bar = c->pk_bar;
+  a.err = c->d_err;  // read back by the next fine residual's norm check
+  a.k = k;
+  // RISM3D_PK_TRACE=1: time every phase (synchronises; diagnostics only)
+  static const int trace_level = [] {
+    const char *t = std::getenv("RISM3D_PK_TRACE");
+    return t ? std::atoi(t) : 0;
+  }();
+  const bool trace = trace_level > 0, trace_steps = trace_level > 1;
+  const int nts = 5 * k + 4;
+  if (trace && !c->pk_trace) c->pk_trace = dalloc<unsigned long long>((size_t)nts);
+  a.trace = trace ? c->pk_trace : nullptr;
+  const cudaError_t e = coarse_pk_launch(a, cc->g.M, cc->g.N1, c->pk_grid, c->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    c->pk_failed = true;
+    c->pk_grid = 0;
+    return false;
+  }
+  if (trace) {
+    std::vector<unsigned long long> ts(nts);
+    CK(cudaMemcpyAsync(ts.data(), c->pk_trace, sizeof(unsigned long long) * nts, cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    // phases: P0, then per step XF Y Z YI XI, then the last update, then the sum
+    double ph[7] = {0, 0, 0, 0, 0, 0, 0};
+    ph[0] = (double)(ts[1] - ts[0]);
+    for (int j = 0; j < k; ++j)
+      for (int p = 0; p < 5; ++p) ph[1 + p] += (double)(ts[2 + 5 * j + p] - ts[1 + 5 * j + p]);
+    ph[6] = (double)(ts[5 * k + 3] - ts[5 * k + 1]);
+    std::fprintf(stderr,
+                 "pk trace (us): total %.1f  P0 %.1f  XF %.1f  Y %.1f  Z %.1f  YI %.1f  XI %.1f  last+sum %.1f "
+                 "(grid %d)\n",
+                 (ts[5 * k + 3] - ts[0]) * 1e-3, ph[0] * 1e-3, ph[1] * 1e-3, ph[2] * 1e-3, ph[3] * 1e-3,
+                 ph[4] * 1e-3, ph[5] * 1e-3, ph[6] * 1e-3, c->pk_grid);
+    if (trace_steps) {
+      for (int j = 0; j < k; ++j) {
+        std::fprintf(stderr, "  step %2d:", j);
+        for (int p = 0; p < 5; ++p) std::fprintf(stderr, " %6.2f", (ts[2 + 5 * j + p] - ts[1 + 5 * j + p]) * 1e-3);
+        std::fprintf(stderr, "\n");
+      }
+    }
+  }
+  return true;
+}
+
 // z = M^-1 (s v).
 template <typename T> void tg_apply(rism3d_ctx *c, const T *v, double s, T *z) {
   rism3d_ctx *cc = c->coarse;
   const int prec = sizeof(T) == 8 ? 0 : 1;
   const int k = coarse_steps(c);
-  const bool graph = coarse_graph(c, k);
   const long long l0 = launch_total(cc);
   {
     TimeScope ts(c, TK_PREC, prec, 6);
-    if (graph) {
+    bool done = false;
+    if (coarse_pk_ready(c, k)) {
+      tg_restrict<T>(c, v, s, basis<float>(cc)[0]);
+      done = coarse_pk_run(c, k);
+      if (done) {
+        c->timer.launches[TK_PREC + 6 * prec] += 1;
+        c->coarse_jv += k;
+      }
+    }
+    const bool graph = !done && coarse_graph(c, k);
+    c->coarse_driver = done ? 2 : (graph ? 1 : 0);
+    if (done) {
+    } else if (graph) {
       tg_restrict<T>(c, v, s, basis<float>(cc)[0]);
       CK(cudaGraphLaunch(c->cg_exec, c->stream));
       c->timer.launches[TK_PREC + 6 * prec] += c->cg_nodes;
@@ -3089,6 +3216,7 @@ int rism3d_solve_batch(int m, const rism3d_site *solvent, int njobs, rism3d_job 
   auto work = [&] {
     // each worker issues on its own per-thread default stream
     if (cudaSetDevice(dev) != cudaSuccess) return;
+    tl_concurrent_solves = nw > 1;
     for (;;) {
       const int i = next.fetch_add(1);
       if (i >= njobs) break;
@@ -3194,6 +3322,11 @@ int rism3d_coarse_grid(rism3d_ctx *ctx, int *n) {
   if (!ctx || !n) return RISM3D_ERR_ARG;
   for (int a = 0; a < 3; ++a) n[a] = ctx->coarse ? ctx->Nc[a] : 0;
   return RISM3D_OK;
+}
+
+int rism3d_coarse_driver(rism3d_ctx *ctx) {
+  if (!ctx) return RISM3D_ERR_ARG;
+  return ctx->coarse_driver;
 }
 
 // ---- profiling hooks (per-pass CUDA-event timing, off by default) -------

@@ -397,6 +397,12 @@ class RismContext:
         _abi.check(_abi.lib().rism3d_coarse_grid(self._h, n), "coarse_grid")
         return None if n[0] == 0 else (n[0], n[1], n[2])
 
+    def coarse_driver(self):
+        """How the last coarse solve ran (rism3d_coarse_driver): "persistent",
+        "graph", "host" or None before the first."""
+        r = _abi.lib().rism3d_coarse_driver(self._h)
+        return {2: "persistent", 1: "graph", 0: "host"}.get(r)
+
     def precondition(self, T, v, out=None):
         """Two-grid preconditioner at state T: M^-1 v (FP64 device tensors)."""
         t = self._torch

@@ -320,6 +320,15 @@ int rism3d_tile_shapes(rism3d_ctx *ctx, int *out);
    n[3] (zeros when the preconditioner is off). */
 int rism3d_coarse_grid(rism3d_ctx *ctx, int *n);
 
+/* How the last coarse solve of the preconditioner ran (diagnostics; no
+   counterpart in the reference): 2 = one persistent cooperative kernel
+   (cubic coarse grids of 48, 64, 72, 96 or 128 points, m <= 3, coarse_steps
+   <= 16, one solve per process at a time), 1 = a replayed CUDA graph of the
+   step-by-step kernels, 0 = host-driven GMRES, -1 = none yet.
+   RISM3D_COARSE_PERSIST=0 / RISM3D_COARSE_GRAPH=0 (environment, read when
+   a context first solves) turn the first two off. */
+int rism3d_coarse_driver(rism3d_ctx *ctx);
+
 /* Per-pass CUDA-event timing (diagnostics): on != 0 enables it (it
    synchronises after every pass, so it is for measurement only).  The
    totals accumulated since the last call are returned in ms[12] /

@@ -182,3 +182,65 @@ def test_fft_transfers_match_dense_long_rows(fixture_loader, N, L, monkeypatch):
         ctx.close()
     for z in out[:2]:
         assert np.max(np.abs(z - out[2])) < 1e-4 * np.max(np.abs(out[2]))
+
+
+@pytest.mark.parametrize("n", [96, 128])
+def test_persistent_coarse_solve(fixture_loader, n, monkeypatch):
+    """The coarse GMRES as one persistent cooperative kernel (coarse grids
+    48^3 and 64^3 of a 48 A box) equals the NumPy restatement and the
+    graph-replayed step-by-step kernels, and repeats bitwise."""
+    meta, arr = fixture_loader("synth6_kh_n32")
+    steps = 16
+    s = settings_of(meta, N=n, L=24.0, **{"coarse-steps": steps})
+    rng = np.random.default_rng(12)
+    out = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("RISM3D_COARSE_PERSIST", mode)
+        ctx = RismContext(meta["solute"], meta["solvent"], s, arr["chi"])
+        nc = ctx.coarse_grid()
+        if not out:
+            T = 0.3 * rng.standard_normal(ctx.shape)
+            v = rng.standard_normal(ctx.shape)
+        z = ctx.precondition(to_dev(T), to_dev(v)).cpu().numpy()
+        z2 = ctx.precondition(to_dev(T), to_dev(v)).cpu().numpy()
+        out[mode] = (z, z2, ctx.coarse_driver(), nc)
+        ctx.close()
+    assert out["1"][2] == "persistent" and out["0"][2] == "graph"
+    assert np.array_equal(out["1"][0], out["1"][1])
+    nc = out["1"][3]
+    assert nc[0] == (48 if n == 96 else 64)
+    R, Pm = transfer(n, nc[0])
+    Pc = problem(meta, arr["chi"], nc[0], L=24.0)
+    P = problem(meta, arr["chi"], n, L=24.0)
+    d = cl.closure1(int(meta["settings"]["closure"]), meta["settings"]["beta"], P.v, T, np.ones_like(T))
+    dH = along(R, d)
+
+    def JH(u):
+        return Pc.ifft(Pc.star(Pc.fft(dH * u) * Pc.h3)) * (1.0 / Pc.L3) - u
+
+    rc = along(R, v)
+    z_ref = along(Pm, gmres_steps(JH, rc, steps) + rc) - v
+    scale = np.max(np.abs(z_ref))
+    for mode in ("1", "0"):
+        assert np.max(np.abs(out[mode][0] - z_ref)) < 1e-4 * scale, mode
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_persistent_coarse_solve_reaches_the_root(fixture_loader, precision, monkeypatch):
+    """Solves with the persistent coarse kernel (128^3, coarse 64^3) reach the
+    same root as with the graph-replayed coarse solve."""
+    meta, arr = fixture_loader("synth6_kh_n32")
+    s = settings_of(meta, N=128, L=24.0, **{"norm-tol": 1e-11, "precision": precision})
+    res = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("RISM3D_COARSE_PERSIST", mode)
+        ctx = RismContext(meta["solute"], meta["solvent"], s, arr["chi"])
+        T, r = ctx.solve()
+        obs = ctx.observables(T)
+        res[mode] = (T.cpu().numpy(), r, obs["free-energy"], ctx.coarse_driver())
+        ctx.close()
+    assert res["1"][3] == "persistent" and res["0"][3] == "graph"
+    for mode in ("1", "0"):
+        assert res[mode][1]["status"] == 0 and res[mode][1]["resid-inf"] < 1e-11
+    assert abs(res["1"][2] - res["0"][2]) < 1e-8
+    assert np.max(np.abs(res["1"][0] - res["0"][0])) < 1e-9
