@@ -21,6 +21,12 @@ this package restates its algorithm in NumPy/SciPy:
 
 Parity is pinned against the reference's published values: README:16
 (1D water mu = -7.869294), README:28/30 (3D water mu = -6.349052 with
-renormalisation, -6.297170 without) and test/out/run-ions-out (3D ions,
-six closures).  See tests/test_oracle_goldens.py.
+renormalisation, -6.297170 without), test/out/water.hnc3d.g2 and the six
+test/out/*.hnc3d.g1 (3D pure solvent and solutes, every printed digit).
+The charged-ion regression test/out/run-ions-out (9 ions x 6 closures, 1D
+and 3D) is reproduced up to one constant per closure and dimension, the
+same for every ion (|offset| < 2.5e-3 in 1D, < 3e-2 in 3D, from the
+long-range treatment of the revision that printed it); after removing it
+every ion agrees to the 4 printed decimals.  See
+tests/test_oracle_goldens.py.
 """
