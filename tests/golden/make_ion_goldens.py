@@ -12,7 +12,8 @@ norm-tol 1e-14.  Nine JC08 ions x six closures (KH, PSE1, PSE2, PSE3,
 PSE7, HNC), 1D and 3D.  The reference's printed values (4 decimals) are
 parsed from run-ions-out; the oracle's come from oracle.rism1d.rism_uv and
 an oracle 3D solve (residual ||F||_inf below TOL3D, the tightest FP64
-reaches for these charged solutes).
+reaches for these charged solutes); the chi of every closure goes to
+tests/golden/ions_chi.npz.
 """
 import json
 import os
@@ -30,6 +31,10 @@ from oracle import closures as cl  # noqa: E402
 from oracle import hnc3d, newton, rism1d  # noqa: E402
 
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ions_regression.json")
+# The oracle's chi per closure: the 3D mu of a charged solute moves by up to
+# 1e-2 kcal/mol when chi changes by 1e-10 near k = 0 (the renormalised
+# long-range term divides by k^2), so parity tests solve on exactly this chi.
+OUT_CHI = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ions_chi.npz")
 NAMES = ["Li+, JC08, SPC/E", "Na+, JC08, SPC/E", "K+, JC08, SPC/E", "Rb+, JC08, SPC/E", "Cs+, JC08, SPC/E",
          "F-, JC08, SPC/E", "Cl-, JC08, SPC/E", "Br-, JC08, SPC/E", "I-, JC08, SPC/E"]
 CLOSURES = ["KH", "PSE1", "PSE2", "PSE3", "PSE7", "HNC"]
@@ -63,10 +68,12 @@ def main():
            "reference": ref, "oracle": {"RISM-1D": {}, "RISM-3D": {}}}
     N = (s["N"],) * 3
     L = (2 * s["L"],) * 3
+    chis = {}
     for clo in CLOSURES:
         c = cl.NAMES[clo]
         chi = rism1d.rism_vv(c, s["nrad"], s["rmax"], s["beta"], s["rho"], solvent, eps=s["dielectric"],
                              tol=1e-12)["chi"]
+        chis[clo] = chi
         res["oracle"]["RISM-1D"][clo] = {}
         res["oracle"]["RISM-3D"][clo] = {}
         for name in NAMES:
@@ -84,6 +91,7 @@ def main():
                   flush=True)
     with open(OUT, "w") as f:
         json.dump(res, f, indent=1)
+    np.savez_compressed(OUT_CHI, **chis)
 
 
 if __name__ == "__main__":
