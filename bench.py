@@ -406,7 +406,7 @@ def pass_bytes(grid, m, b, launches, f_evals):
 def run_ours(args, rank, world):
     import torch
     import torch.distributed as dist
-    from bgy3d_b200 import RismContext, hnc3d_run_solute
+    from bgy3d_b200 import RismContext, hnc3d_run_solute, lib
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
@@ -467,14 +467,19 @@ def run_ours(args, rank, world):
     one(ctx)
     prof = ctx.profile(False)
 
-    # end to end through the host-buffer C-ABI call (hnc3d_run_solute)
+    # end to end through the host-buffer C-ABI call (hnc3d_run_solute): one
+    # untimed call (it builds the device context the later calls reuse),
+    # then k timed calls, each with its host arrays, solute upload, solve,
+    # observables and the copy of g into host memory
     torch.cuda.synchronize()
-    k_e2e = max(1, min(args.steps, 2))
+    hnc3d_run_solute(solute, solvent, dict(s, precision="mixed"), chi, want_g=True, want_restart=False)
+    k_e2e = max(1, min(args.steps, 3))
     t0 = time.perf_counter()
     for _ in range(k_e2e):
         out = hnc3d_run_solute(solute, solvent, dict(s, precision="mixed"), chi, want_g=True,
                                want_restart=False)
     e2e_s = (time.perf_counter() - t0) / k_e2e
+    lib().rism3d_cache_clear()
     ctx.close()
     if rank != 0:
         return None
@@ -525,8 +530,11 @@ def run_ours(args, rank, world):
                      "share_of_solve": sum(pms.values()) / total_ms, "pass_gbs": pass_gbs,
                      "passes_ms": {f"{a}/{p}": round(v[0], 3) for (a, p), v in prof.items() if v[1]}},
         "e2e": {"value": 1.0 / e2e_s, "unit": "solves/s",
-                "h2d_bytes_per_step": int(chi.nbytes + 2 * 64 * (N_SITES + 3)),
-                "d2h_bytes_per_step": int(out["GUV"].nbytes)},
+                "h2d_bytes_per_step": int(48 * N_SITES),
+                "d2h_bytes_per_step": int(out["GUV"].nbytes), "calls": k_e2e,
+                "timing": "host clock around hnc3d_run_solute (rism3d_solute_solve with host buffers): solute "
+                          "upload, solve from t = 0, observables, g copied into a fresh host array; the device "
+                          "context of the untimed first call is reused (the solute rebound)"},
         "gpu_launches": int(launches),
     }
     if clocks:

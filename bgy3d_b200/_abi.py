@@ -97,7 +97,7 @@ EXPORTS = [
     "rism3d_solute_grad", "rism3d_gradient", "rism3d_jacobian_transpose_t1", "rism3d_ctx_set_solute",
     "rism3d_response", "rism3d_solvent_solve", "rism3d_solvent_ctx_create", "rism3d_ctx_create_chi3",
     "rism3d_solute_solve_chi3", "rism3d_info", "rism3d_moments", "rism3d_tile_shapes",
-    "rism3d_free_energy_gradient",
+    "rism3d_free_energy_gradient", "rism3d_cache_clear",
 ]
 
 _lib = None
@@ -148,6 +148,8 @@ def lib():
     L.rism3d_coarse_grid.restype = I
     L.rism3d_coarse_driver.argtypes = [V]
     L.rism3d_coarse_driver.restype = I
+    L.rism3d_cache_clear.argtypes = []
+    L.rism3d_cache_clear.restype = None
     L.rism3d_solve_batch.argtypes = [I, P(Site), I, P(Job), I]
     L.rism3d_solve_batch.restype = I
     L.rism3d_solute_grad.argtypes = [P(Problem), I, P(Site), I, P(Site), P(D), P(D), P(Result), P(Grad)]

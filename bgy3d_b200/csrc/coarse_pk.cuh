@@ -63,6 +63,7 @@ struct PkArgs {
   int *err;              // set to kPkErr on a barrier timeout
   int k;                 // GMRES steps, 1 .. kPkMaxSteps
   unsigned long long *trace;  // diagnostics, or null: %globaltimer at the start and at every barrier (CTA 0)
+  unsigned long long *trace_cta;  // diagnostics, or null: [barrier][2][grid] arrival / release of every CTA
 };
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
@@ -80,11 +81,13 @@ __device__ __forceinline__ unsigned long long global_ns() {
 }
 
 __device__ __forceinline__ bool grid_sync(unsigned *bar, unsigned gen, int *err,
-                                          unsigned long long *trace = nullptr) {
+                                          unsigned long long *trace = nullptr,
+                                          unsigned long long *trace_cta = nullptr) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
+    if (trace_cta) trace_cta[(size_t)(gen - 1) * 2 * gridDim.x + blockIdx.x] = global_ns();
     // arrive with release semantics (the CTA's writes, ordered before this
     // thread by the barrier above, become visible first), then poll with
     // acquire loads: the first load that sees every arrival orders all later
@@ -102,6 +105,7 @@ __device__ __forceinline__ bool grid_sync(unsigned *bar, unsigned gen, int *err,
     if (!ok) atomicCAS(err, 0, kPkErr);
     s_ok = ok;
     if (trace && blockIdx.x == 0) trace[gen] = global_ns();
+    if (trace_cta) trace_cta[(size_t)(gen - 1) * 2 * gridDim.x + gridDim.x + blockIdx.x] = global_ns();
   }
   __syncthreads();
   return s_ok != 0;
@@ -122,11 +126,13 @@ __device__ __forceinline__ void pk_sum_partials(const double *part, int stride, 
   }
   red[threadIdx.x] = s;
   __syncthreads();
-  if ((int)threadIdx.x < nv) {
-    double t = 0.0;
-    for (int r = 0; r < groups; ++r) t += red[r * lanes + threadIdx.x];
-    out[threadIdx.x] = t;
+  // pairwise over the groups (slot q * lanes + v keeps v): log2(groups)
+  // steps instead of a chain of `groups` dependent adds
+  for (int stride = kPkThreads / 2; stride >= lanes; stride >>= 1) {
+    if ((int)threadIdx.x < stride) red[threadIdx.x] += red[threadIdx.x + stride];
+    __syncthreads();
   }
+  if ((int)threadIdx.x < nv) out[threadIdx.x] = red[threadIdx.x];
   __syncthreads();
 }
 
@@ -513,7 +519,7 @@ __global__ void __launch_bounds__(kPkThreads, 2) k_coarse_gmres(PkArgs a) {
     }
     pk_block_sum(s2, a.pnrm);
   }
-  if (!grid_sync(a.bar, ++gen, a.err, a.trace)) return;
+  if (!grid_sync(a.bar, ++gen, a.err, a.trace, a.trace_cta)) return;
   pk_sum_partials(a.pnrm, 1, gridDim.x, 1, sD);
   if (tid == 0) sS[0] = sqrt(fmax(sD[0], 0.0));
   __syncthreads();
@@ -533,7 +539,7 @@ __global__ void __launch_bounds__(kPkThreads, 2) k_coarse_gmres(PkArgs a) {
     }
     pk_xf<M>(a, sV, j, j, sC, j < k, tile, twx, nrm2);
     if (j > 0) pk_block_sum(nrm2, a.pnrm + (j & 1) * gridDim.x);
-    if (!grid_sync(a.bar, ++gen, a.err, a.trace)) return;
+    if (!grid_sync(a.bar, ++gen, a.err, a.trace, a.trace_cta)) return;
     if (j > 0) {
       pk_sum_partials(a.pnrm + (j & 1) * gridDim.x, 1, gridDim.x, 1, sD);
       if (tid == 0) {
@@ -544,11 +550,11 @@ __global__ void __launch_bounds__(kPkThreads, 2) k_coarse_gmres(PkArgs a) {
     }
     if (j == k) break;
     pk_y<N, false>(a, tile, twy);
-    if (!grid_sync(a.bar, ++gen, a.err, a.trace)) return;
+    if (!grid_sync(a.bar, ++gen, a.err, a.trace, a.trace_cta)) return;
     pk_z<N>(a, tile, twz);
-    if (!grid_sync(a.bar, ++gen, a.err, a.trace)) return;
+    if (!grid_sync(a.bar, ++gen, a.err, a.trace, a.trace_cta)) return;
     pk_y<N, true>(a, tile, twy);
-    if (!grid_sync(a.bar, ++gen, a.err, a.trace)) return;
+    if (!grid_sync(a.bar, ++gen, a.err, a.trace, a.trace_cta)) return;
     // V_{j+1} = J (V_j / s_j) = (X / N - V_j) / s_j
     const double sj = sS[j];
     const float inv = sj > 0.0 ? (float)(1.0 / sj) : 0.f;
@@ -561,7 +567,7 @@ __global__ void __launch_bounds__(kPkThreads, 2) k_coarse_gmres(PkArgs a) {
       for (int w = 0; w < kPkThreads / 32; ++w) t += sdot[tid][w];
       a.pdot[(long long)blockIdx.x * kVecMax + tid] = t;
     }
-    if (!grid_sync(a.bar, ++gen, a.err, a.trace)) return;
+    if (!grid_sync(a.bar, ++gen, a.err, a.trace, a.trace_cta)) return;
   }
 
   // least squares (every CTA, bitwise alike), then out = sum_j y_j V_j / s_j

@@ -425,8 +425,13 @@ __global__ void __launch_bounds__(256) k_xinv(Geo g, AxisPlan px, int RX,
 // ============================================================ setup fields
 struct SiteP { double x, y, z, sigma, epsilon, charge; };
 
-__device__ __forceinline__ double lj0(double r) { const double p6 = pow(r, -6.0); return 4 * p6 * (p6 - 1); }
-__device__ __forceinline__ double lj1(double r) { const double p6 = pow(r, -6.0); return 4 * p6 * (6 - 12 * p6) / r; }
+// r^-6 as (1/r^2)^3: one division instead of a general pow (a few ulp apart)
+__device__ __forceinline__ double inv_pow6(double r) {
+  const double i2 = 1.0 / (r * r);
+  return i2 * i2 * i2;
+}
+__device__ __forceinline__ double lj0(double r) { const double p6 = inv_pow6(r); return 4 * p6 * (p6 - 1); }
+__device__ __forceinline__ double lj1(double r) { const double p6 = inv_pow6(r); return 4 * p6 * (6 - 12 * p6) / r; }
 __device__ __forceinline__ double ljcap0(double r) {   // bgy3d-solutes.c:101-114
   const double R = 0.2;
   if (r >= R) return lj0(r);
@@ -451,7 +456,56 @@ __device__ __forceinline__ double cl0(double r) {     // bgy3d-solutes.c:147-159
 }
 
 // v[i][p] = sum_u eps_iu ljcap0(r/sigma_iu) + q_i q_u/eps0 G cscap0(G r)
-// (field0, bgy3d-solutes.c:343-377); grid point r = i h - L/2.
+// (field0, bgy3d-solutes.c:343-377); grid point r = i h - L/2.  The pair
+// constants (eps_iu, sigma_iu, q_i q_u / eps0) and the solute positions sit
+// in shared memory ([n][m][3] then [n][3] doubles, kField0MaxPairs pairs at
+// most); the capped Coulomb value of a solute site is evaluated once per
+// point and shared by all solvent sites.  Same terms, same order as the
+// direct form below.
+constexpr int kField0MaxPairs = 1536;
+static __global__ void __launch_bounds__(256) k_field0_pairs(Geo g, double h0, double h1, double h2, double L0,
+                                                             double L1, double L2, const SiteP *__restrict__ solvent,
+                                                             int n, const SiteP *__restrict__ solute,
+                                                             double *__restrict__ v) {
+  extern __shared__ double sp[];
+  const int m = g.m;
+  double *sx = sp + 3 * n * m;
+  for (int e = threadIdx.x; e < n * m; e += blockDim.x) {
+    const int u = e / m, s = e - u * m;
+    const SiteP a = solvent[s], b = solute[u];
+    sp[3 * e] = sqrt(a.epsilon * b.epsilon);
+    sp[3 * e + 1] = 0.5 * (a.sigma + b.sigma);
+    sp[3 * e + 2] = a.charge * b.charge * kEps0Inv;
+  }
+  for (int u = threadIdx.x; u < n; u += blockDim.x) {
+    sx[3 * u] = solute[u].x;
+    sx[3 * u + 1] = solute[u].y;
+    sx[3 * u + 2] = solute[u].z;
+  }
+  __syncthreads();
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= g.Nr) return;
+  const int i0 = (int)(p % g.N0);
+  const int i1 = (int)((p / g.N0) % g.N1);
+  const int i2 = (int)(p / ((long long)g.N0 * g.N1));
+  const double x = i0 * h0 - L0 / 2, y = i1 * h1 - L1 / 2, z = i2 * h2 - L2 / 2;
+  double e[kMaxSites];
+#pragma unroll
+  for (int s = 0; s < kMaxSites; ++s) e[s] = 0.0;
+  for (int u = 0; u < n; ++u) {
+    const double dx = x - sx[3 * u], dy = y - sx[3 * u + 1], dz = z - sx[3 * u + 2];
+    const double rab = sqrt(dx * dx + dy * dy + dz * dz);
+    const double cs = cscap0(kG * rab);
+    const double *c = sp + 3 * u * m;
+#pragma unroll
+    for (int s = 0; s < kMaxSites; ++s)
+      if (s < m) e[s] += c[3 * s] * ljcap0(rab / c[3 * s + 1]) + c[3 * s + 2] * kG * cs;
+  }
+#pragma unroll
+  for (int s = 0; s < kMaxSites; ++s)
+    if (s < m) v[(long long)s * g.Nr + p] = e[s];
+}
+
 static __global__ void k_field0(Geo g, double h0, double h1, double h2, double L0, double L1, double L2,
                          const SiteP *__restrict__ solvent, int n, const SiteP *__restrict__ solute,
                          double *__restrict__ v) {
@@ -495,12 +549,29 @@ static __global__ void k_coulomb_long(Geo g, double h0, double h1, double h2, do
   uc[p] = kEps0Inv * s;
 }
 
+// Per-axis phase factors of the solute form factor: tab[u][i] = exp(-i k_a(i)
+// x_{u,a}) for axis a, i < n_a (k_a(i) = kfreq(i, Nfull_a) dk_a); so that
+// exp(-i k.x_u) = tab0[u][ix] tab1[u][iy] tab2[u][iz].
+static __global__ void k_phase_axis(int n, int na, int nfull, double dk, int axis, const SiteP *__restrict__ solute,
+                                    double2 *__restrict__ tab) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n * na) return;
+  const int u = e / na, i = e - u * na;
+  const double xu = axis == 0 ? solute[u].x : (axis == 1 ? solute[u].y : solute[u].z);
+  double sn, cs;
+  sincos(kfreq(i, nfull) * dk * xu, &sn, &cs);
+  tab[e] = make_double2(cs, -sn);
+}
+
 // Long-range k-field, centred (bgy3d_solute_form, bgy3d-solutes.c:633-698):
 // F(k) = sum_u q_u exp(-i k.x_u) (-1)^(kx+ky+kz).  renorm: L = F / h^3;
 // no-renorm: L = (4 pi/eps0) exp(-k^2/4G^2)/k^2 F / h^3 (coulomb_long_fft,
-// bgy3d-solutes.c:766-792; zero at k = 0).  Written in FP64 and FP32.
-static __global__ void k_longrange(Geo g, int n, const SiteP *__restrict__ solute, int renorm, double inv_h3,
-                            double2 *__restrict__ L64, float2 *__restrict__ L32) {
+// bgy3d-solutes.c:766-792; zero at k = 0).  Written in FP64 and FP32.  The
+// phase of site u is the product of its three per-axis factors (k_phase_axis).
+static __global__ void k_longrange_tab(Geo g, int n, const SiteP *__restrict__ solute,
+                                       const double2 *__restrict__ t0, const double2 *__restrict__ t1,
+                                       const double2 *__restrict__ t2, int renorm, double inv_h3,
+                                       double2 *__restrict__ L64, float2 *__restrict__ L32) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long tot = (long long)g.Nh * g.N1 * g.N2;
   if (p >= tot) return;
@@ -508,18 +579,18 @@ static __global__ void k_longrange(Geo g, int n, const SiteP *__restrict__ solut
   const int iy = (int)((p / g.Nh) % g.N1);
   const int iz = (int)(p / ((long long)g.Nh * g.N1));
   const int fx = kfreq(ix, g.N0), fy = kfreq(iy, g.N1), fz = kfreq(iz, g.N2);
-  const double k0 = fx * g.dk0, k1 = fy * g.dk1, k2 = fz * g.dk2;
   double re = 0.0, im = 0.0;
   for (int u = 0; u < n; ++u) {
-    const double ph = (k0 * solute[u].x + k1 * solute[u].y) + k2 * solute[u].z;
-    double sn, cs;
-    sincos(ph, &sn, &cs);
-    re += solute[u].charge * cs;
-    im -= solute[u].charge * sn;
+    const double2 a = t0[(long long)u * g.Nh + ix], b = t1[(long long)u * g.N1 + iy], c = t2[(long long)u * g.N2 + iz];
+    const double br = a.x * b.x - a.y * b.y, bi = a.x * b.y + a.y * b.x;
+    const double q = solute[u].charge;
+    re += q * (br * c.x - bi * c.y);
+    im += q * (br * c.y + bi * c.x);
   }
   const int sgn = (((fx % 2) != 0) ^ ((fy % 2) != 0) ^ ((fz % 2) != 0)) ? -1 : 1;
   double f = sgn * inv_h3;
   if (!renorm) {
+    const double k0 = fx * g.dk0, k1 = fy * g.dk1, k2 = fz * g.dk2;
     const double kk = (k0 * k0 + k1 * k1) + k2 * k2;
     f *= kk == 0.0 ? 0.0 : (4 * M_PI * kEps0Inv) * exp(-kk / (4 * kG * kG)) / kk;
   }

@@ -267,7 +267,10 @@ struct rism3d_ctx {
   int pk_grid = 0;                              // CTAs (0: not set up)
   bool pk_failed = false;                       // shape or device without it
   int coarse_driver = -1;  // of the last coarse solve: 0 host-driven, 1 graph, 2 persistent kernel
+  double2 *phase_tab = nullptr;  // per-axis phase factors of the solute form factor [3 axes][phase_cap][n_a]
+  int phase_cap = 0;
   unsigned long long *pk_trace = nullptr;       // RISM3D_PK_TRACE: phase timestamps
+  unsigned long long *pk_trace_cta = nullptr;   // RISM3D_PK_TRACE=3: every CTA at every barrier
 
   cudaStream_t stream = 0;
   PassTimer timer;
@@ -294,7 +297,7 @@ struct rism3d_ctx {
     for (auto p : zbasis32) fr(p);
     for (int a = 0; a < 3; ++a) { fr(tR[a]); fr(tRt[a]); fr(tP[a]); fr(tPt[a]); }
     fr(tA); fr(tB); fr(tc_r); fr(tc_y); fr(cg_H); fr(cg_aux); fr(cg_ticket); fr(tC); fr(tD);
-    fr(pk_dot); fr(pk_nrm); fr(pk_bar); fr(pk_trace);
+    fr(pk_dot); fr(pk_nrm); fr(pk_bar); fr(pk_trace); fr(pk_trace_cta); fr(phase_tab);
     if (cg_exec) cudaGraphExecDestroy(cg_exec);
     if (cg_graph) cudaGraphDestroy(cg_graph);
     delete coarse;
@@ -1176,6 +1179,11 @@ bool coarse_pk_run(rism3d_ctx *c, int k) {
   const int nts = 5 * k + 4;
   if (trace && !c->pk_trace) c->pk_trace = dalloc<unsigned long long>((size_t)nts);
   a.trace = trace ? c->pk_trace : nullptr;
+  const int nbar = 5 * k + 2;
+  const bool trace_ctas = trace_level > 2;
+  if (trace_ctas && !c->pk_trace_cta)
+    c->pk_trace_cta = dalloc<unsigned long long>((size_t)nbar * 2 * c->pk_grid);
+  a.trace_cta = trace_ctas ? c->pk_trace_cta : nullptr;
   const cudaError_t e = coarse_pk_launch(a, cc->g.M, cc->g.N1, c->pk_grid, c->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -1199,6 +1207,37 @@ bool coarse_pk_run(rism3d_ctx *c, int k) {
                  "(grid %d)\n",
                  (ts[5 * k + 3] - ts[0]) * 1e-3, ph[0] * 1e-3, ph[1] * 1e-3, ph[2] * 1e-3, ph[3] * 1e-3,
                  ph[4] * 1e-3, ph[5] * 1e-3, ph[6] * 1e-3, c->pk_grid);
+    if (trace_ctas) {
+      // per phase type: CTA work time (arrival - own previous release),
+      // median and max over CTAs and steps; arrival spread (last - first
+      // arrival); release lag (last release - last arrival)
+      const int G = c->pk_grid;
+      std::vector<unsigned long long> tc((size_t)nbar * 2 * G);
+      CK(cudaMemcpy(tc.data(), c->pk_trace_cta, sizeof(unsigned long long) * tc.size(), cudaMemcpyDeviceToHost));
+      const char *names[5] = {"XF", "Y", "Z", "YI", "XI"};
+      for (int p = 0; p < 5; ++p) {
+        std::vector<double> work;
+        double spread = 0, lag = 0, lagmax = 0;
+        for (int j = 0; j < k; ++j) {
+          const int b = 1 + 5 * j + p;  // barrier index (0-based) closing this phase
+          unsigned long long amin = ~0ull, amax = 0, rmax = 0;
+          for (int q = 0; q < G; ++q) {
+            const unsigned long long arr = tc[(size_t)b * 2 * G + q], prev = tc[(size_t)(b - 1) * 2 * G + G + q];
+            work.push_back((double)(arr - prev));
+            amin = std::min(amin, arr);
+            amax = std::max(amax, arr);
+            rmax = std::max(rmax, tc[(size_t)b * 2 * G + G + q]);
+          }
+          spread += (double)(amax - amin);
+          lag += (double)(rmax - amax);
+          lagmax = std::max(lagmax, (double)(rmax - amax));
+        }
+        std::sort(work.begin(), work.end());
+        std::fprintf(stderr, "  %-2s work median %.2f p90 %.2f max %.2f | arrival spread %.2f | release lag %.2f (max %.2f) us\n",
+                     names[p], work[work.size() / 2] * 1e-3, work[work.size() * 9 / 10] * 1e-3, work.back() * 1e-3,
+                     spread / k * 1e-3, lag / k * 1e-3, lagmax * 1e-3);
+      }
+    }
     if (trace_steps) {
       for (int j = 0; j < k; ++j) {
         std::fprintf(stderr, "  step %2d:", j);
@@ -1855,16 +1894,36 @@ void bind_solute(rism3d_ctx *c, int n, const rism3d_site *solute) {
   c->solute.assign(solute, solute + n);
   const double h0 = pd.L[0] / pd.N[0], h1 = pd.L[1] / pd.N[1], h2 = pd.L[2] / pd.N[2];
   const unsigned nb = (unsigned)((G.Nr + 255) / 256);
-  k_field0<<<nb, 256, 0, c->stream>>>(G, h0, h1, h2, pd.L[0], pd.L[1], pd.L[2], c->d_solvent, n, c->d_solute,
-                                      c->v64);
+  if (n * G.m <= kField0MaxPairs && n <= 512) {
+    const size_t sm = sizeof(double) * (size_t)(3 * n * G.m + 3 * n);
+    k_field0_pairs<<<nb, 256, sm, c->stream>>>(G, h0, h1, h2, pd.L[0], pd.L[1], pd.L[2], c->d_solvent, n,
+                                               c->d_solute, c->v64);
+  } else {
+    k_field0<<<nb, 256, 0, c->stream>>>(G, h0, h1, h2, pd.L[0], pd.L[1], pd.L[2], c->d_solvent, n, c->d_solute,
+                                        c->v64);
+  }
   CKL();
   k_axpby<double, float><<<vec_grid(c->nvec), 256, 0, c->stream>>>(c->nvec, 1.0, c->v64, 0.0, c->v32);
   CKL();
   CK(cudaMemsetAsync(c->L64, 0, sizeof(double2) * (size_t)G.Nhp * G.N1 * G.N2, c->stream));
   CK(cudaMemsetAsync(c->L32, 0, sizeof(float2) * (size_t)G.Nhp * G.N1 * G.N2, c->stream));
   const long long nk = (long long)G.Nh * G.N1 * G.N2;
-  k_longrange<<<(unsigned)((nk + 255) / 256), 256, 0, c->stream>>>(G, n, c->d_solute, pd.renorm, 1.0 / c->h3,
-                                                                   c->L64, c->L32);
+  // per-axis phase tables of the solute form factor, then the k-field
+  const size_t per = (size_t)G.Nh + G.N1 + G.N2;
+  if (!c->phase_tab || n > c->phase_cap) {
+    dfree(c->phase_tab);
+    c->phase_cap = std::max(n, 1);
+    c->phase_tab = dalloc<double2>((size_t)c->phase_cap * per);
+  }
+  double2 *t0 = c->phase_tab, *t1 = t0 + (size_t)c->phase_cap * G.Nh, *t2 = t1 + (size_t)c->phase_cap * G.N1;
+  if (n > 0) {
+    k_phase_axis<<<(n * G.Nh + 255) / 256, 256, 0, c->stream>>>(n, G.Nh, G.N0, G.dk0, 0, c->d_solute, t0);
+    k_phase_axis<<<(n * G.N1 + 255) / 256, 256, 0, c->stream>>>(n, G.N1, G.N1, G.dk1, 1, c->d_solute, t1);
+    k_phase_axis<<<(n * G.N2 + 255) / 256, 256, 0, c->stream>>>(n, G.N2, G.N2, G.dk2, 2, c->d_solute, t2);
+    CKL();
+  }
+  k_longrange_tab<<<(unsigned)((nk + 255) / 256), 256, 0, c->stream>>>(G, n, c->d_solute, t0, t1, t2, pd.renorm,
+                                                                       1.0 / c->h3, c->L64, c->L32);
   CKL();
   CK(cudaStreamSynchronize(c->stream));  // hs is freed on return
   if (c->coarse) bind_solute(c->coarse, n, solute);
@@ -2950,6 +3009,136 @@ void d2h_large(void *dst, const void *src, size_t bytes, cudaStream_t st) {
   }
 }
 
+// Contexts of finished host-buffer solves, kept for the next
+// rism3d_solute_solve with the same device, problem settings, solvent and
+// chi: that call rebinds the solute (its short-range field and long-range
+// term) instead of building the context again -- the grids, chi tables,
+// coarse problem, transfer tables, Krylov buffers and the captured coarse
+// solve are reused, as FFT plan caches reuse plans.  At most
+// RISM3D_CTX_CACHE contexts (default 1, 0: off) are kept, least recently
+// used first out; rism3d_cache_clear() frees them.  A context is taken out
+// of the cache while a solve runs on it, so concurrent callers never share
+// one.
+struct CacheKey {
+  int dev = -1;
+  rism3d_problem pd{};
+  std::vector<rism3d_site> solvent;
+  std::vector<double> chi;  // [m][m][nrad]
+};
+struct CacheEntry {
+  CacheKey key;
+  rism3d_ctx *ctx;
+};
+std::mutex g_cache_mu;
+std::vector<CacheEntry> g_cache;  // most recently used last
+
+size_t cache_capacity() {
+  static const size_t cap = [] {
+    const char *e = std::getenv("RISM3D_CTX_CACHE");
+    return e ? (size_t)std::max(0, std::atoi(e)) : size_t(1);
+  }();
+  return cap;
+}
+
+bool same_problem(const rism3d_problem &a, const rism3d_problem &b) {
+  for (int i = 0; i < 3; ++i)
+    if (a.N[i] != b.N[i] || a.L[i] != b.L[i]) return false;
+  return a.beta == b.beta && a.rho == b.rho && a.rmax == b.rmax && a.nrad == b.nrad && a.closure == b.closure &&
+         a.max_iter == b.max_iter && a.norm_tol == b.norm_tol && a.lambda == b.lambda && a.solver == b.solver &&
+         a.renorm == b.renorm && a.precision == b.precision && a.verbosity == b.verbosity &&
+         a.krylov_restart == b.krylov_restart && a.ew_forcing == b.ew_forcing && a.coarse_h == b.coarse_h &&
+         a.coarse_steps == b.coarse_steps;
+}
+
+bool same_sites(const rism3d_site *a, const rism3d_site *b, int n) {
+  for (int i = 0; i < n; ++i)
+    if (a[i].x[0] != b[i].x[0] || a[i].x[1] != b[i].x[1] || a[i].x[2] != b[i].x[2] || a[i].sigma != b[i].sigma ||
+        a[i].epsilon != b[i].epsilon || a[i].charge != b[i].charge)
+      return false;
+  return true;
+}
+
+rism3d_ctx *cache_take(const rism3d_problem *pd, int m, const rism3d_site *solvent, const double *chi) {
+  if (cache_capacity() == 0) return nullptr;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  const size_t nchi = (size_t)m * m * (size_t)std::max(pd->nrad, 0);
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  for (size_t i = g_cache.size(); i-- > 0;) {
+    const CacheKey &k = g_cache[i].key;
+    if (k.dev != dev || (int)k.solvent.size() != m || k.chi.size() != nchi || !same_problem(k.pd, *pd) ||
+        !same_sites(k.solvent.data(), solvent, m) || std::memcmp(k.chi.data(), chi, sizeof(double) * nchi) != 0)
+      continue;
+    rism3d_ctx *c = g_cache[i].ctx;
+    g_cache.erase(g_cache.begin() + (long)i);
+    return c;
+  }
+  return nullptr;
+}
+
+void cache_put(rism3d_ctx *c, const rism3d_problem *pd, int m, const rism3d_site *solvent, const double *chi) {
+  const size_t cap = cache_capacity();
+  int dev = 0;
+  if (cap == 0 || cudaGetDevice(&dev) != cudaSuccess) {
+    delete c;
+    return;
+  }
+  CacheEntry e{CacheKey{}, c};
+  e.key.dev = dev;
+  e.key.pd = *pd;
+  e.key.solvent.assign(solvent, solvent + m);
+  e.key.chi.assign(chi, chi + (size_t)m * m * (size_t)std::max(pd->nrad, 0));
+  std::vector<rism3d_ctx *> drop;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    g_cache.push_back(std::move(e));
+    while (g_cache.size() > cap) {
+      drop.push_back(g_cache.front().ctx);
+      g_cache.erase(g_cache.begin());
+    }
+  }
+  for (auto *d : drop) delete d;
+}
+
+void cache_clear() {
+  std::vector<CacheEntry> all;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    all.swap(g_cache);
+  }
+  for (auto &e : all) delete e.ctx;
+}
+
+// Writes one byte into every page of [p, p + bytes) from a few host threads:
+// a caller's fresh result buffer (a NumPy array) takes its first-touch page
+// faults here, while the device solves, instead of inside the copy-out.
+struct PageToucher {
+  std::vector<std::thread> th;
+  PageToucher(void *p, size_t bytes) {
+    if (!p || bytes < (size_t(64) << 20)) return;
+    const long pg = 4096;
+    const int nthr = 4;
+    const size_t slice = (bytes / nthr + pg - 1) / pg * pg;
+    for (int q = 0; q < nthr; ++q) {
+      const size_t a = std::min(bytes, q * slice), b = std::min(bytes, (q + 1) * slice);
+      if (a >= b) continue;
+      try {
+        th.emplace_back([=] {
+          volatile char *c = static_cast<char *>(p);
+          for (size_t o = a; o < b; o += pg) c[o] = 0;
+        });
+      } catch (const std::system_error &) {
+        break;  // no thread: the copy-out takes the faults
+      }
+    }
+  }
+  void join() {
+    for (auto &t : th) t.join();
+    th.clear();
+  }
+  ~PageToucher() { join(); }
+};
+
 int solve_on(rism3d_ctx *ctx, double *t_inout, double *g_out, rism3d_result *out) {
   const size_t bytes = sizeof(double) * ctx->nvec;
   double *T = dalloc<double>(ctx->nvec);
@@ -2957,11 +3146,13 @@ int solve_on(rism3d_ctx *ctx, double *t_inout, double *g_out, rism3d_result *out
   struct Free { double *a, *b; ~Free() { dfree(a); dfree(b); } } fr{T, g};
   if (t_inout) CK(cudaMemcpy(T, t_inout, bytes, cudaMemcpyHostToDevice));
   else CK(cudaMemset(T, 0, bytes));
+  PageToucher touch(g_out, bytes);  // g_out is written in full below; its old contents do not matter
   rism3d_result r{};
   int st = solve_impl(ctx, T, &r);
   observables_impl(ctx, T, g, &r);
   r.launches += 2;  // the observables' kernels
   r.status = st;
+  touch.join();
   if (t_inout) d2h_large(t_inout, T, bytes, ctx->stream);
   if (g_out) d2h_large(g_out, g, bytes, ctx->stream);
   if (out) *out = r;
@@ -3110,17 +3301,38 @@ int rism3d_get_field(rism3d_ctx *ctx, int which, double *dst) {
 int rism3d_solute_solve(const rism3d_problem *pd, int m, const rism3d_site *solvent, int n,
                         const rism3d_site *solute, const double *chi, double *t_inout, double *g_out,
                         rism3d_result *out) {
+  int rc = RISM3D_OK;
   rism3d_ctx *ctx = nullptr;
-  int rc = rism3d_ctx_create(pd, m, solvent, n, solute, chi, &ctx);
-  if (rc != RISM3D_OK) {
-    if (out) { std::memset(out, 0, sizeof(*out)); out->status = rc; }
-    return rc;
+  if (pd && solvent && chi && m >= 1 && m <= kMaxSites && n >= 0 && (solute || n == 0)) {
+    ctx = cache_take(pd, m, solvent, chi);
+    if (ctx) {
+      rc = guard([&] {
+        bind_solute(ctx, n, solute);
+        return (int)RISM3D_OK;
+      });
+      if (rc != RISM3D_OK) {
+        delete ctx;
+        ctx = nullptr;
+      }
+    }
+  }
+  if (!ctx) {
+    rc = rism3d_ctx_create(pd, m, solvent, n, solute, chi, &ctx);
+    if (rc != RISM3D_OK) {
+      if (out) { std::memset(out, 0, sizeof(*out)); out->status = rc; }
+      return rc;
+    }
   }
   rc = guard([&] { return solve_on(ctx, t_inout, g_out, out); });
-  rism3d_ctx_destroy(ctx);
+  if (rc == RISM3D_OK || rc == RISM3D_ERR_NOT_CONVERGED || rc == RISM3D_ERR_NAN)
+    cache_put(ctx, pd, m, solvent, chi);
+  else
+    rism3d_ctx_destroy(ctx);
   if (out && rc < 0 && out->status == 0) out->status = rc;
   return rc;
 }
+
+void rism3d_cache_clear(void) { cache_clear(); }
 
 int rism3d_tile_shapes(rism3d_ctx *ctx, int *out) {
   if (!ctx || !out) return RISM3D_ERR_ARG;

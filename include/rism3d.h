@@ -134,6 +134,15 @@ void rism3d_problem_defaults(rism3d_problem *pd, double L_half, int N);
              token of hnc3d.c:1830-1845, 2301-2316.
     g_out    host [m][N2][N1][N0] or NULL: g = h + 1 (hnc3d.c:2320, 2341).
     out      results; out->status repeats the return code.
+
+  The device context of a finished call (grids, chi tables, the
+  preconditioner's coarse problem, Krylov buffers) is kept for the next
+  call on the same device with equal problem settings, solvent sites and
+  chi contents, which then only rebinds the solute -- the PES loop of
+  guile/bgy3d.scm:819-880 calling this repeatedly pays the set-up once.
+  At most RISM3D_CTX_CACHE contexts (environment, read once; default 1,
+  0 turns the cache off) stay allocated between calls; concurrent calls
+  never share one.
 */
 int rism3d_solute_solve(const rism3d_problem *pd,
                         int m, const rism3d_site *solvent,
@@ -141,6 +150,10 @@ int rism3d_solute_solve(const rism3d_problem *pd,
                         const double *chi,
                         double *t_inout, double *g_out,
                         rism3d_result *out);
+
+/* Frees the contexts rism3d_solute_solve keeps between calls (no
+   counterpart in the reference, which builds its context on every call). */
+void rism3d_cache_clear(void);
 
 /* Derivatives of the free energy mu (the closure's native functional) with
    respect to the solute's site parameters, and diagnostics of the adjoint
