@@ -41,6 +41,9 @@ using namespace rism;
 
 namespace rism {  // twogrid_fx2.cu: x transfers with both sides by FFT
 bool fx2_has_pair(int M, int MC);
+// twogrid_yz.cu: y / z transfers by FFT
+bool yz_fft_transfer(int outer, int n_in, int n_out, int inner, const float *in, const float2 *twi,
+                     const float2 *two, float *out, cudaStream_t st);
 // coarse_pk.cu: the persistent cooperative coarse GMRES
 int coarse_pk_grid(int M, int N, int per_sm);
 cudaError_t coarse_pk_launch(const PkArgs &a, int M, int N, int grid, cudaStream_t st);
@@ -876,11 +879,25 @@ long long launch_total(const rism3d_ctx *c) {
   return s;
 }
 
-// Slab width J of the y / z transfers: 32 outputs per thread for the
-// restrictions (n_out <= 64: the input is read at most twice), 16 for the
-// prolongations, 8 where the threads of a narrow slab would not fill the GPU.
-void transfer_axis(rism3d_ctx *c, int outer, int n_in, int n_out, int inner, const float *in, const float *A,
-                   float *out) {
+// The y (axis 1) or z (axis 2) transfer of [outer][n_in][inner] into
+// [outer][n_out][inner]: by FFT (twogrid_yz.cu) where that pair of lengths
+// has a kernel, else as the dense product with A (RISM3D_DENSE_TRANSFERS=1
+// forces the dense form, for the comparison tests).  Slab width J of the
+// dense form: 32 outputs per thread for the restrictions (n_out <= 64: the
+// input is read at most twice), 16 for the prolongations, 8 where the
+// threads of a narrow slab would not fill the GPU.
+void transfer_axis(rism3d_ctx *c, int axis, int outer, int n_in, int n_out, int inner, const float *in,
+                   const float *A, float *out) {
+  const char *dense = std::getenv("RISM3D_DENSE_TRANSFERS");
+  if (!(dense && dense[0] == '1')) {
+    const float2 *tw_fine = c->tw32[axis], *tw_coarse = c->coarse->tw32[axis];
+    const bool restrict_ = n_out < n_in;
+    if (rism::yz_fft_transfer(outer, n_in, n_out, inner, in, restrict_ ? tw_fine : tw_coarse,
+                              restrict_ ? tw_coarse : tw_fine, out, c->stream)) {
+      CKL();
+      return;
+    }
+  }
   const long long tot = (long long)outer * inner;
   const unsigned gx = (unsigned)((tot + tg::kAxThreads - 1) / tg::kAxThreads);
   int J = n_out <= 64 ? 32 : 16;
@@ -991,15 +1008,15 @@ template <typename T> void tg_restrict(rism3d_ctx *c, const T *in, double s, flo
     tg::k_restrict_x<T><<<gx, tg::kRxThreads, 0, c->stream>>>(rows, G.N0, c->Nc[0], in, (float)s, c->tRt[0], c->tA);
     CKL();
   }
-  transfer_axis(c, c->m * G.N2, G.N1, c->Nc[1], c->Nc[0], c->tA, c->tR[1], c->tB);
-  transfer_axis(c, c->m, G.N2, c->Nc[2], c->Nc[1] * c->Nc[0], c->tB, c->tR[2], out);
+  transfer_axis(c, 1, c->m * G.N2, G.N1, c->Nc[1], c->Nc[0], c->tA, c->tR[1], c->tB);
+  transfer_axis(c, 2, c->m, G.N2, c->Nc[2], c->Nc[1] * c->Nc[0], c->tB, c->tR[2], out);
 }
 
 // out = P yc - s r (fine), yc coarse.
 template <typename T> void tg_prolong(rism3d_ctx *c, const float *yc, const T *r, double s, T *out) {
   const Geo &G = c->g;
-  transfer_axis(c, c->m, c->Nc[2], G.N2, c->Nc[1] * c->Nc[0], yc, c->tP[2], c->tB);
-  transfer_axis(c, c->m * G.N2, c->Nc[1], G.N1, c->Nc[0], c->tB, c->tP[1], c->tA);
+  transfer_axis(c, 2, c->m, c->Nc[2], G.N2, c->Nc[1] * c->Nc[0], yc, c->tP[2], c->tB);
+  transfer_axis(c, 1, c->m * G.N2, c->Nc[1], G.N1, c->Nc[0], c->tB, c->tP[1], c->tA);
   const long long rows = (long long)c->m * G.N2 * G.N1;
   if (!fx_prolong<T>(c, rows, r, s, out)) {
     dim3 gx((unsigned)((rows + tg::kPxRows - 1) / tg::kPxRows), (unsigned)((G.N0 + tg::kPxCols - 1) / tg::kPxCols));
