@@ -72,14 +72,14 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
   return v;
 }
 
-// Grid barrier number `gen` (1, 2, ...): done when the counter reaches
-// gen * gridDim.x.  CTA-uniform result; false: leave the kernel.
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
 
+// Grid barrier number `gen` (1, 2, ...): done when the counter reaches
+// gen * gridDim.x.  CTA-uniform result; false: leave the kernel.
 __device__ __forceinline__ bool grid_sync(unsigned *bar, unsigned gen, int *err,
                                           unsigned long long *trace = nullptr,
                                           unsigned long long *trace_cta = nullptr) {
@@ -150,6 +150,10 @@ __device__ __forceinline__ void pk_block_sum(double s, double *part) {
   }
 }
 
+// The split of the x-phase transforms (measured: the larger first radix of
+// Split beats SplitRow at 48-row items of 32-point rows).
+template <int M> using PkSplit = Split<M>;
+
 // Rows of the x phases per work item: about one item per CTA of a 2 x 148
 // grid for m = 3, a multiple of 8, at most 4 float4 of a vector per thread.
 template <int M> __host__ __device__ constexpr int pk_rx() {
@@ -168,7 +172,7 @@ template <int M>
 __device__ __forceinline__ void pk_xf(const PkArgs &a, float *const *V, int j, int nu, const float *cf, bool fft,
                                       float2 *buf, const float2 *tw, double &nrm2) {
   constexpr int RX = pk_rx<M>();
-  using Lay = LayRow<M, Split<M>::R2>;
+  using Lay = LayRow<M, PkSplit<M>::R2>;
   constexpr int PER_ROW = M / 2;  // float4 per row (two complex values)
   constexpr int CNT = (RX * PER_ROW + kPkThreads - 1) / kPkThreads;
   constexpr int H = M / 2 + 1;
@@ -241,7 +245,7 @@ __device__ __forceinline__ void pk_xf(const PkArgs &a, float *const *V, int j, i
       buf[Lay::at(jj + 1, row)] = z1;
     }
     __syncthreads();
-    fft2<M, RX, kPkThreads, false, false, Lay>(buf, tw);
+    fft2<M, RX, kPkThreads, false, false, Lay, PkSplit<M>>(buf, tw);
     for (int e = tid; e < RX * H; e += kPkThreads) {
       const int row = e / H, kk = e % H;
       const int grow = row0 + row;
@@ -269,7 +273,7 @@ template <int M>
 __device__ __forceinline__ void pk_xi(const PkArgs &a, float *const *V, int j, float sc, float sub, float2 *buf,
                                       const float2 *tw, double (*sdot)[kPkThreads / 32]) {
   constexpr int RX = pk_rx<M>();
-  using Lay = LayRow<M, Split<M>::R2>;
+  using Lay = LayRow<M, PkSplit<M>::R2>;
   constexpr int PER_ROW = M / 2;
   constexpr int CNT = (RX * PER_ROW + kPkThreads - 1) / kPkThreads;
   constexpr int GV = pk_group<CNT>();
@@ -311,7 +315,7 @@ __device__ __forceinline__ void pk_xi(const PkArgs &a, float *const *V, int j, f
       if (kk != 0 && M - kk != kk) buf[Lay::at(M - kk, row)] = zm;
     }
     __syncthreads();
-    fft2<M, RX, kPkThreads, true, false, Lay>(buf, tw);
+    fft2<M, RX, kPkThreads, true, false, Lay, PkSplit<M>>(buf, tw);
     float4 o[CNT];
 #pragma unroll
     for (int it = 0; it < CNT; ++it) {
@@ -476,7 +480,7 @@ __device__ __forceinline__ void pk_lsq(int k, double *H, double beta, double *y,
 // Shared memory of the phases (dynamic part): the three twiddle tables and
 // the largest work tile.
 template <int M, int N> __host__ __device__ constexpr size_t pk_smem() {
-  constexpr size_t xs = (size_t)pk_rx<M>() * (M + M / Split<M>::R2);
+  constexpr size_t xs = (size_t)pk_rx<M>() * LayRow<M, PkSplit<M>::R2>::RS;
   constexpr size_t ys = (size_t)(kPkThreads / (Split<N>::R1 * 16)) * N * 16;
   constexpr size_t zs = (size_t)(kPkThreads / (Split<N>::R1 * kPkBz * 3)) * 3 * N * kPkBz;
   constexpr size_t tile = xs > ys ? (xs > zs ? xs : zs) : (ys > zs ? ys : zs);

@@ -82,6 +82,15 @@ template <int N> struct Split {
   static constexpr int R2 = N / R1;
 };
 
+// The split of the row-batched transforms (x passes and x transfers: one
+// work item per row and index, COLFAST false), where Split's larger first
+// radix would leave most of the CTA idle in one step (32 = 16 x 2 gives R2 x
+// rows items of 16-point DFTs); here both steps keep the CTA busy.
+template <int N> struct SplitRow {
+  static constexpr int R1 = N == 24 ? 6 : N == 32 ? 8 : N == 36 ? 6 : N == 48 ? 8 : N == 96 ? 12 : Split<N>::R1;
+  static constexpr int R2 = N / R1;
+};
+
 // Tile layouts: element (i, col) of the transform index i and column col.
 // Columns fastest, [n][B] tiles of NB per sub-tile stacked SB times
 // ([s][n][b], the TMA boxes of the y and z passes):
@@ -89,9 +98,14 @@ template <int N, int B> struct LayCol {
   __device__ __forceinline__ static int at(int i, int col) { return (col / B) * (N * B) + i * B + (col % B); }
 };
 // Rows of N with one pad element every R2 (the x pass), keeping the strided
-// accesses of both steps off a single bank:
+// accesses of both steps off a single bank, and the row stride RS = R2 mod
+// 16 complex values: in step 1 a warp spans 32 / R2 rows of R2 consecutive
+// work items each, which then fall on disjoint banks instead of piling onto
+// the same ones (a stride that is a multiple of 32 banks made 128-point rows
+// 4-way conflicted).
 template <int N, int R2> struct LayRow {
-  static constexpr int RS = N + N / R2;
+  static constexpr int RS0 = N + N / R2;
+  static constexpr int RS = RS0 + ((R2 % 16) - RS0 % 16 + 16) % 16;
   __device__ __forceinline__ static int at(int i, int row) { return row * RS + i + i / R2; }
 };
 
@@ -101,9 +115,10 @@ template <int N, int R2> struct LayRow {
 // consecutive threads to consecutive columns (column-contiguous tiles),
 // otherwise to consecutive transform indices (row-contiguous tiles).  Ends
 // synchronised.
-template <int N, int NCOL, int NTHR, bool INV, bool COLFAST, class Lay, typename V>
+template <int N, int NCOL, int NTHR, bool INV, bool COLFAST, class Lay, class S = Split<N>, typename V>
 __device__ __forceinline__ void fft2g(V *buf, const V *tw, int tid, bool act) {
-  constexpr int R1 = Split<N>::R1, R2 = Split<N>::R2;
+  constexpr int R1 = S::R1, R2 = S::R2;
+  static_assert(R1 * R2 == N, "split must factor N");
   constexpr int I1 = R2 * NCOL;
 #pragma unroll
   for (int it = 0; it < (I1 + NTHR - 1) / NTHR; ++it) {
@@ -156,9 +171,9 @@ __device__ __forceinline__ void fft2g(V *buf, const V *tw, int tid, bool act) {
   __syncthreads();
 }
 // The whole CTA as one group of NTHR threads.
-template <int N, int NCOL, int NTHR, bool INV, bool COLFAST, class Lay, typename V>
+template <int N, int NCOL, int NTHR, bool INV, bool COLFAST, class Lay, class S = Split<N>, typename V>
 __device__ __forceinline__ void fft2(V *buf, const V *tw) {
-  fft2g<N, NCOL, NTHR, INV, COLFAST, Lay>(buf, tw, (int)threadIdx.x, true);
+  fft2g<N, NCOL, NTHR, INV, COLFAST, Lay, S>(buf, tw, (int)threadIdx.x, true);
 }
 
 // ------------------------------------------------------------- TMA + mbarrier

@@ -29,7 +29,7 @@ __global__ void __launch_bounds__(256) k_xfwd_s(Geo g, const T *__restrict__ A, 
                                                const typename Cx<T>::type *__restrict__ post,
                                                const typename Cx<T>::type *__restrict__ twg) {
   using V = typename Cx<T>::type;
-  using Lay = LayRow<M, Split<M>::R2>;
+  using Lay = LayRow<M, SplitRow<M>::R2>;
   constexpr int VW = VecW<T>::n;
   using VEC = typename VecW<T>::vec;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(256) k_xfwd_s(Geo g, const T *__restrict__ A, 
     for (int v = 0; v < VW; ++v) buf[Lay::at(jj + v, row)] = z[v];
   }
   __syncthreads();
-  fft2<M, RX, 256, false, false, Lay>(buf, tw);
+  fft2<M, RX, 256, false, false, Lay, SplitRow<M>>(buf, tw);
   constexpr int H = M / 2 + 1;
   const long long wbase = (long long)site * g.Nc;
   for (int e = tid; e < RX * H; e += 256) {
@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(256) k_xinv_s(Geo g, const typename Cx<T>::typ
                                                const typename Cx<T>::type *__restrict__ twg,
                                                NormPartial *__restrict__ part) {
   using V = typename Cx<T>::type;
-  using Lay = LayRow<M, Split<M>::R2>;
+  using Lay = LayRow<M, SplitRow<M>::R2>;
   constexpr int VW = VecW<T>::n;
   using VEC = typename VecW<T>::vec;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(256) k_xinv_s(Geo g, const typename Cx<T>::typ
     }
   }
   __syncthreads();
-  fft2<M, RX, 256, true, false, Lay>(buf, tw);
+  fft2<M, RX, 256, true, false, Lay, SplitRow<M>>(buf, tw);
   double amax = 0.0, sum2 = 0.0;
 #pragma unroll
   for (int it = 0; it < CNT; ++it) {

@@ -393,7 +393,7 @@ constexpr int kStaticRX = 16;
 template <typename T> constexpr int static_B() { return sizeof(T) == 4 ? 16 : 8; }
 template <typename T> constexpr int static_Bz() { return sizeof(T) == 4 ? 8 : 4; }
 template <typename T, int M> constexpr size_t xs_smem() {
-  return sizeof(typename Cx<T>::type) * (size_t)(M + kStaticRX * (M + M / Split<M>::R2));
+  return sizeof(typename Cx<T>::type) * (size_t)(M + kStaticRX * LayRow<M, SplitRow<M>::R2>::RS);
 }
 template <typename T, int N> constexpr size_t ys_smem() {
   return sizeof(typename Cx<T>::type) * (size_t)(N * static_B<T>() + N) + 16;

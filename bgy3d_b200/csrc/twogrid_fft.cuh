@@ -26,7 +26,7 @@ template <> __device__ __forceinline__ float2 ld_pair<double>(const double *p) {
   return make_float2((float)v.x, (float)v.y);
 }
 
-template <int M, int RX> __host__ __device__ constexpr int fx_buf() { return RX * LayRow<M, Split<M>::R2>::RS; }
+template <int M, int RX> __host__ __device__ constexpr int fx_buf() { return RX * LayRow<M, SplitRow<M>::R2>::RS; }
 
 // Shared memory of the two kernels (bytes) for K = Nc/2: twiddles, the row
 // tiles, the coarse-side table, the kept spectrum (and the coarse rows).
@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(256) k_restrict_fx(long long rows, int Nc, int
                                                      const float2 *__restrict__ twg,
                                                      const float2 *__restrict__ ctab, float *__restrict__ out) {
   using V = float2;
-  using Lay = LayRow<M, Split<M>::R2>;
+  using Lay = LayRow<M, SplitRow<M>::R2>;
   using Q = typename Quad<TI>::type;
   constexpr int N0 = 2 * M, PER = M / 2, CNT = (RX * PER + 255) / 256;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(256) k_restrict_fx(long long rows, int Nc, int
     }
     if (bat + gridDim.x < nbat) FX_LOAD_ROWS(bat + gridDim.x)
     __syncthreads();
-    fft2<M, RX, 256, false, false, Lay>(buf, tw);
+    fft2<M, RX, 256, false, false, Lay, SplitRow<M>>(buf, tw);
     for (int e = tid; e < RX * K1; e += 256) {
       const int row = e / K1, k = e - row * K1;
       const V zk = buf[Lay::at(k, row)];
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(256) k_prolong_fx(long long rows, int Nc, int 
                                                     const float2 *__restrict__ dtab, const TR *__restrict__ r,
                                                     double s, TO *__restrict__ out) {
   using V = float2;
-  using Lay = LayRow<M, Split<M>::R2>;
+  using Lay = LayRow<M, SplitRow<M>::R2>;
   using QR = typename Quad<TR>::type;
   constexpr int N0 = 2 * M, H = M / 2 + 1, PER = M / 2, CNT = (RX * PER + 255) / 256;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(256) k_prolong_fx(long long rows, int Nc, int 
       if (k != 0 && M - k != k) buf[Lay::at(M - k, row)] = zm;
     }
     __syncthreads();
-    fft2<M, RX, 256, true, false, Lay>(buf, tw);
+    fft2<M, RX, 256, true, false, Lay, SplitRow<M>>(buf, tw);
 #pragma unroll
     for (int it = 0; it < CNT; ++it) {
       const int e = tid + it * 256;
@@ -333,8 +333,8 @@ __global__ void __launch_bounds__(256) k_restrict_fx2(long long rows, const TI *
                                                       const float2 *__restrict__ postc,
                                                       const float2 *__restrict__ twcg, float *__restrict__ out) {
   using V = float2;
-  using Lay = LayRow<M, Split<M>::R2>;
-  using LayC = LayRow<MC, Split<MC>::R2>;
+  using Lay = LayRow<M, SplitRow<M>::R2>;
+  using LayC = LayRow<MC, SplitRow<MC>::R2>;
   using Q = typename Quad<TI>::type;
   static_assert(MC < M && fx_buf<MC, RX>() <= fx_buf<M, RX>(), "coarse row tile must fit the fine one");
   constexpr int N0 = 2 * M, Nc = 2 * MC, K = MC, K1 = MC + 1;
@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(256) k_restrict_fx2(long long rows, const TI *
     }
     if (bat + gridDim.x < nbat) FX2_LOAD_ROWS(bat + gridDim.x)
     __syncthreads();
-    fft2<M, RX, 256, false, false, Lay>(buf, tw);
+    fft2<M, RX, 256, false, false, Lay, SplitRow<M>>(buf, tw);
     for (int e = tid; e < RX * K1; e += 256) {
       const int row = e / K1, k = e - row * K1;
       const V zk = buf[Lay::at(k, row)];
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(256) k_restrict_fx2(long long rows, const TI *
     __syncthreads();
     fx_pack_c2r<MC, RX, LayC>(X, K, K1, postc, buf);
     __syncthreads();
-    fft2<MC, RX, 256, true, false, LayC>(buf, twc);
+    fft2<MC, RX, 256, true, false, LayC, SplitRow<MC>>(buf, twc);
     for (int e = tid; e < RX * PC; e += 256) {
       const int row = e / PC, jj = (e - row * PC) * 2;
       if (row0 + row >= rows) continue;
@@ -411,14 +411,14 @@ __global__ void __launch_bounds__(256) k_restrict_fx2(long long rows, const TI *
 // unbounded choice of 128 registers only 2 fit; the bound costs a few spilled
 // words there (more at 256-point rows, which keep the unbounded choice)
 template <typename TO, typename TR, int M, int MC, int RX>
-__global__ void __launch_bounds__(256, M == 128 ? 3 : 1) k_prolong_fx2(long long rows, const float *__restrict__ y,
+__global__ void __launch_bounds__(256, M == 128 ? (RX >= 32 ? 2 : 3) : 1) k_prolong_fx2(long long rows, const float *__restrict__ y,
                                                      const float2 *__restrict__ post, const float2 *__restrict__ twg,
                                                      const float2 *__restrict__ postc,
                                                      const float2 *__restrict__ twcg, const TR *__restrict__ r,
                                                      double s, TO *__restrict__ out) {
   using V = float2;
-  using Lay = LayRow<M, Split<M>::R2>;
-  using LayC = LayRow<MC, Split<MC>::R2>;
+  using Lay = LayRow<M, SplitRow<M>::R2>;
+  using LayC = LayRow<MC, SplitRow<MC>::R2>;
   using QR = typename Quad<TR>::type;
   static_assert(MC < M && fx_buf<MC, RX>() <= fx_buf<M, RX>(), "coarse row tile must fit the fine one");
   constexpr int N0 = 2 * M, Nc = 2 * MC, K = MC, K1 = MC + 1;
@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(256, M == 128 ? 3 : 1) k_prolong_fx2(long long
     const bool more = bat + gridDim.x < nbat;
     if (more) FX2_LOAD(bat + gridDim.x, rn)
     __syncthreads();
-    fft2<MC, RX, 256, false, false, LayC>(buf, twc);
+    fft2<MC, RX, 256, false, false, LayC, SplitRow<MC>>(buf, twc);
     // untangle to the Nc-point r2c, weights f_k (1/Nc, half at the Nyquist K)
     for (int e = tid; e < RX * K1; e += 256) {
       const int row = e / K1, k = e - row * K1;
@@ -486,7 +486,7 @@ __global__ void __launch_bounds__(256, M == 128 ? 3 : 1) k_prolong_fx2(long long
     __syncthreads();
     fx_pack_c2r<M, RX, Lay>(X, K, K1, post, buf);
     __syncthreads();
-    fft2<M, RX, 256, true, false, Lay>(buf, tw);
+    fft2<M, RX, 256, true, false, Lay, SplitRow<M>>(buf, tw);
 #pragma unroll
     for (int it = 0; it < CNT; ++it) {
       const int e = tid + it * 256;

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "twogrid_fft.cuh"
 
@@ -15,6 +16,16 @@ namespace rism {
 namespace {
 
 constexpr int kRX = 16;  // rows per batch, as the table-product kernels
+
+// Rows per batch of the 128-point half rows (the 256^3 grid): 16 or 32
+// (RISM3D_FX2_ROWS, read once).
+int rows_128() {
+  static const int r = [] {
+    const char *e = std::getenv("RISM3D_FX2_ROWS");
+    return e && std::atoi(e) == 32 ? 32 : 16;
+  }();
+  return r;
+}
 
 // Persistent CTAs: as many as fit at once, at most `work`; also raises the
 // kernel's dynamic shared-memory limit when it needs more than 48 KB.
@@ -51,6 +62,19 @@ bool fx2_has_pair(int M, int MC) {
 template <typename T>
 bool fx2_restrict(int M, int MC, long long rows, const T *in, float s, const float2 *post, const float2 *tw,
                   const float2 *postc, const float2 *twc, float *out, cudaStream_t st) {
+  if (M == 128 && rows_128() == 32) {
+    const unsigned nb32 = (unsigned)((rows + 31) / 32);
+#define FX2_R32(A, B)                                                                                       \
+  if (MC == B) {                                                                                            \
+    const size_t sm = fx2_smem<A, B, 32>();                                                                 \
+    const unsigned g = fx2_grid((const void *)k_restrict_fx2<T, A, B, 32>, sm, nb32);                       \
+    if (g == 0) return false;                                                                               \
+    k_restrict_fx2<T, A, B, 32><<<g, 256, sm, st>>>(rows, in, s, post, tw, postc, twc, out);                \
+    return true;                                                                                            \
+  }
+    FX2_R32(128, 32) FX2_R32(128, 48) FX2_R32(128, 64)
+#undef FX2_R32
+  }
   const unsigned nb = (unsigned)((rows + kRX - 1) / kRX);
 #define FX2_R(A, B)                                                                                         \
   if (M == A && MC == B) {                                                                                  \
@@ -69,6 +93,19 @@ bool fx2_restrict(int M, int MC, long long rows, const T *in, float s, const flo
 template <typename T>
 bool fx2_prolong(int M, int MC, long long rows, const float *y, const float2 *post, const float2 *tw,
                  const float2 *postc, const float2 *twc, const T *r, double s, T *out, cudaStream_t st) {
+  if (M == 128 && rows_128() == 32) {
+    const unsigned nb32 = (unsigned)((rows + 31) / 32);
+#define FX2_P32(A, B)                                                                                       \
+  if (MC == B) {                                                                                            \
+    const size_t sm = fx2_smem<A, B, 32>();                                                                 \
+    const unsigned g = fx2_grid((const void *)k_prolong_fx2<T, T, A, B, 32>, sm, nb32);                     \
+    if (g == 0) return false;                                                                               \
+    k_prolong_fx2<T, T, A, B, 32><<<g, 256, sm, st>>>(rows, y, post, tw, postc, twc, r, s, out);            \
+    return true;                                                                                            \
+  }
+    FX2_P32(128, 32) FX2_P32(128, 48) FX2_P32(128, 64)
+#undef FX2_P32
+  }
   const unsigned nb = (unsigned)((rows + kRX - 1) / kRX);
 #define FX2_P(A, B)                                                                                         \
   if (M == A && MC == B) {                                                                                  \
