@@ -327,8 +327,11 @@ __device__ __forceinline__ void fx_pack_c2r(const float2 *X, int K, int K1, cons
   }
 }
 
+// 128-point half rows at 3 CTAs per SM (80 registers, no spills; the
+// unbounded choice of 128 allows 2): the batches are latency chains, so
+// resident CTAs set the throughput.
 template <typename TI, int M, int MC, int RX>
-__global__ void __launch_bounds__(256) k_restrict_fx2(long long rows, const TI *__restrict__ in, float s,
+__global__ void __launch_bounds__(256, M == 128 ? 3 : 1) k_restrict_fx2(long long rows, const TI *__restrict__ in, float s,
                                                       const float2 *__restrict__ post, const float2 *__restrict__ twg,
                                                       const float2 *__restrict__ postc,
                                                       const float2 *__restrict__ twcg, float *__restrict__ out) {
