@@ -28,7 +28,8 @@ dmu/d(q, sigma, eps, x) of the workload's solute (time against one
 solve, central-difference checks); "pes", an 8-point scan of the solute
 rebound on one context with warm starts, against fresh solves;
 "cufft_yardstick", the Jacobian product against a cuFFT (torch.fft) form of
-it, speed and max difference.
+it, speed and max difference; "large", the 512^3 / 150-site single solve
+below, timed once.
 
   python bench.py --large           the 512^3 / 150-site single solve
                                     (mixed against plain FP64)
@@ -282,8 +283,16 @@ def run_large(args):
     half edge 48 A (96 A box, h = 0.1875 A), mixed precision to |F|inf <
     1e-10 against the plain FP64 form; device time, peak device memory of
     the library's pool and per-pass HBM rates of one mixed solve."""
+    print(json.dumps(large_report()))
+
+
+def large_report():
+    """run_large's measurement as a dict (also the "large" key of the default
+    line, timed once after the timed steps)."""
     import torch
-    from bgy3d_b200 import RismContext, find_molecule, rism_solvent, synthetic_solute
+    from bgy3d_b200 import RismContext, find_molecule, lib, rism_solvent, synthetic_solute
+    lib().rism3d_cache_clear()
+    torch.cuda.empty_cache()
     solvent = find_molecule("water, PR-SPC/E")
     solute = synthetic_solute(150, radius=14.0, seed=20261203)
     s = dict(SETTINGS, N=512, L=48.0)
@@ -328,7 +337,7 @@ def run_large(args):
     out["dmu_vs_fp64_plain"] = out["mixed"]["mu"] - out["fp64_plain"]["mu"]
     out["device_memory_note"] = "free device memory before the first context minus after each solve (the pool " \
                                 "keeps its high-water mark)"
-    print(json.dumps(out))
+    return out
 
 
 def config(grid=GRID, precision="mixed"):
@@ -545,7 +554,8 @@ def run_ours(args, rank, world):
         extras = (("batch", lambda: run_batch_report(solvent, s, chi)),
                   ("gradient", lambda: run_gradient_report(solute, solvent, s, chi, ms / args.steps)),
                   ("pes", lambda: run_pes_report(solute, solvent, s, chi)),
-                  ("cufft_yardstick", lambda: run_cufft_yardstick(solute, solvent, dict(s, precision="mixed"), chi)))
+                  ("cufft_yardstick", lambda: run_cufft_yardstick(solute, solvent, dict(s, precision="mixed"), chi)),
+                  ("large", large_report))
         for key, fn in extras:
             try:
                 line[key] = fn()
