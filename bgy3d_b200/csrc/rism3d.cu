@@ -724,6 +724,39 @@ double maxpy(rism3d_ctx *c, T *w, double ws, const std::vector<VecRef<T>> &V, co
   return std::sqrt(hres[0]);
 }
 
+// One classical Gram-Schmidt step of w against s_i V_i (nv <= kVecMax) with
+// a single host round trip: the dots <w, V_i> stay on the device (dres) and
+// feed the update w -= sum_i (s_i^2 <w, V_i>) V_i as device coefficients;
+// the dots and |w|^2 come back together.  h_i = s_i <w, V_i>; returns |w|
+// after the update.
+template <typename T>
+double gs_step(rism3d_ctx *c, T *w, const std::vector<VecRef<T>> &V, std::vector<double> &h) {
+  const int nv = (int)V.size();
+  TimeScope ts(c, TK_VEC, sizeof(T) == 8 ? 0 : 1, 4);
+  const int G = c->red_blocks;
+  const long long nw = c->nvec / Wide<T>::n;
+  VecSet<T> vs{};
+  Coefs cf{};
+  for (int i = 0; i < kVecMax; ++i) {
+    vs.p[i] = V[i < nv ? i : 0].p;
+    cf.c[i] = i < nv ? V[i].s * V[i].s : 0.0;
+  }
+  launch_mdotv<T>(G, c->stream, nw, w, nv, vs, c->dpart);
+  CKL();
+  k_colsum<<<1, kVecMax * 8, 0, c->stream>>>(G, kVecMax, nv, c->dpart, c->dres);
+  CKL();
+  k_maxpyv<T><<<G, 256, 0, c->stream>>>(nw, w, 1.0, nv, vs, cf, c->dres, c->dpart);
+  CKL();
+  k_colsum<<<1, kVecMax * 8, 0, c->stream>>>(G, 1, 1, c->dpart, c->dres + kVecMax);
+  CKL();
+  double *hres = pinned_scratch();
+  CK(cudaMemcpyAsync(hres, c->dres, sizeof(double) * (kVecMax + 1), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  h.assign(nv, 0.0);
+  for (int i = 0; i < nv; ++i) h[i] = hres[i] * V[i].s;
+  return std::sqrt(std::max(hres[kVecMax], 0.0));
+}
+
 template <typename TX, typename TY> void axpby(rism3d_ctx *c, double a, const TX *x, double b, TY *y) {
   TimeScope ts(c, TK_VEC, sizeof(TY) == 8 ? 0 : 1);
   k_axpby<TX, TY><<<vec_grid(c->nvec), 256, 0, c->stream>>>(c->nvec, a, x, b, y);
@@ -783,8 +816,13 @@ int gmres(rism3d_ctx *c, const T *d, T *b, T *x, double rtol, int maxit, int res
     for (; j < restart && its < maxit; ++j) {
       eval_J<T>(c, d, V[j].p, V[j].s, B[j + 1], nullptr);
       its++;
-      mdot<T>(c, B[j + 1], 1.0, V, h);
-      const double hn = maxpy<T>(c, B[j + 1], 1.0, V, h, true);
+      double hn;
+      if ((int)V.size() <= kVecMax) {
+        hn = gs_step<T>(c, B[j + 1], V, h);
+      } else {
+        mdot<T>(c, B[j + 1], 1.0, V, h);
+        hn = maxpy<T>(c, B[j + 1], 1.0, V, h, true);
+      }
       for (int i = 0; i <= j; ++i) H[(size_t)i * restart + j] = h[i];
       H[(size_t)(j + 1) * restart + j] = hn;
       for (int i = 0; i < j; ++i) {  // previous Givens rotations
@@ -1344,8 +1382,13 @@ int fgmres(rism3d_ctx *c, const T *d, T *b, T *x, double rtol, int maxit, int re
       tg_apply<T>(c, V[j].p, V[j].s, Z[j]);
       eval_J<T>(c, d, Z[j], 1.0, B[j + 1], nullptr);
       its++;
-      mdot<T>(c, B[j + 1], 1.0, V, h);
-      const double hn = maxpy<T>(c, B[j + 1], 1.0, V, h, true);
+      double hn;
+      if ((int)V.size() <= kVecMax) {
+        hn = gs_step<T>(c, B[j + 1], V, h);
+      } else {
+        mdot<T>(c, B[j + 1], 1.0, V, h);
+        hn = maxpy<T>(c, B[j + 1], 1.0, V, h, true);
+      }
       for (int i = 0; i <= j; ++i) H[(size_t)i * restart + j] = h[i];
       H[(size_t)(j + 1) * restart + j] = hn;
       for (int i = 0; i < j; ++i) {
