@@ -431,7 +431,7 @@ __device__ __forceinline__ void pk_z(const PkArgs &a, float2 *smem, const float2
       }
     }
     __syncthreads();
-    z_tile_g<float, MODE_J, N, B, MS, true>(g, buf, tw, a.zp, kx0, y, tid, act);
+    z_tile_g<float, MODE_J, N, B, MS, true, 1>(g, buf, tw, a.zp, kx0, y, tid, act);
     if (act) {
       for (int e = tid; e < g.m * N * (B / 2); e += NG) {
         const int s = e / (N * (B / 2)), r = e % (N * (B / 2));

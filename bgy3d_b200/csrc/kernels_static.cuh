@@ -272,36 +272,52 @@ __global__ void __launch_bounds__(Split<N>::R1 * B) k_y_s(Geo g, const __grid_co
   }
 }
 
+// Elements whose chi table entries a thread has in flight during the z
+// contraction: 4 in the FP32 Jacobian pass, 2 where the residual's
+// long-range terms or FP64 values take the registers (the FP32 passes stay
+// within 128 registers, i.e. the 4 CTAs per SM that shared memory allows).
+template <typename T, int MODE> __host__ __device__ constexpr int zpf_default() {
+  return sizeof(T) == 4 && MODE == MODE_J ? 4 : 2;
+}
+
 // One z tile in shared memory: forward transform along z of the m [N][B]
 // site columns, the OZ contraction with the radial chi-1 tables (+ the
 // long-range terms in MODE_F), inverse transform; ends after a barrier.
 // Run by the NTHR = R1 B threads tid of a group (act false: barriers only);
 // JOINT: the MS site tiles (all allocated) transform as one MS B-column
 // tile by R1 B MS threads.
-template <typename T, int MODE, int N, int B, int MS, bool JOINT = false>
+//
+// The contraction is software-pipelined: the table entries of an element
+// depend only on where it sits on the k grid, so a thread keeps those of its
+// next ZPF elements (and, in MODE_F, their long-range values) in flight
+// while it contracts the current one, and issues the first ZPF before the
+// forward transforms, under whose latency they arrive.  Same arithmetic in
+// the same order as contracting element by element.
+template <typename T, int MODE, int N, int B, int MS, bool JOINT = false, int ZPF = zpf_default<T, MODE>()>
 __device__ __forceinline__ void z_tile_g(const Geo &g, typename Cx<T>::type *buf, const typename Cx<T>::type *tw,
                                          const ZParams<T> &zp, int kx0, int y, int tid, bool act) {
   using V = typename Cx<T>::type;
   using P2 = typename Vec2<T>::type;
   constexpr int NTHR = Split<N>::R1 * B * (JOINT ? MS : 1);
+  constexpr int NP = MS * (MS + 1) / 2;
+  constexpr int NIT = (N * B + NTHR - 1) / NTHR;
+  constexpr int D = NIT < ZPF ? NIT : ZPF;
   const int m = g.m;
+  const int np = m * (m + 1) / 2;
   const int bw = min(B, g.Nh - kx0);
-  if (JOINT) fft2g<N, MS * B, NTHR, false, true, LayCol<N, B>>(buf, tw, tid, act);
-  else
-    for (int s = 0; s < m; ++s) fft2g<N, B, NTHR, false, true, LayCol<N, B>>(buf + s * N * B, tw, tid, act);
+  const bool full = MODE == MODE_F && zp.L != nullptr;
   const int ky = kfreq(y, g.N1);
   const double k1 = ky * g.dk1;
   const long long zstride = (long long)g.N1 * g.Nhp;
   const long long col = (long long)y * g.Nhp + kx0;
-  // contraction: all table entries of an element are fetched before use and
-  // two elements are in flight per thread (the tables live in L1/L2)
-  constexpr int NP = MS * (MS + 1) / 2;
-  const int np = m * (m + 1) / 2;
-  const bool full = MODE == MODE_F && zp.L != nullptr;
-#pragma unroll 2
-  for (int e = act ? tid : N * B; e < N * B; e += NTHR) {
+  P2 tq[D][NP];   // chi - 1 (value, slope) of each pair
+  P2 sq[D][MS];   // beta/eps0 s_i (value, slope), MODE_F
+  V lq[D];        // long-range value, MODE_F
+  T fq[D];        // interpolation fraction
+  auto fetch = [&](int it, int slot) {
+    const int e = tid + it * NTHR;
+    if (!act || e >= N * B) return;
     const int z = e / B, b = e % B;
-    const bool valid = b < bw;
     const int kx = kx0 + b;
     const int kz = kfreq(z, N);
     const double k0 = kx * g.dk0, k2 = kz * g.dk2;
@@ -309,57 +325,71 @@ __device__ __forceinline__ void z_tile_g(const Geo &g, typename Cx<T>::type *buf
     const double ix = kk / zp.dkr - 0.5;
     int i = (int)(ix + 0.5);
     i = min(max(i, 0), zp.nrad - 1);
-    const T fr = T(ix - i);
-    P2 tv[NP];
+    fq[slot] = T(ix - i);
 #pragma unroll
     for (int q = 0; q < NP; ++q)
-      if (q < np) tv[q] = __ldg(&zp.chi[(long long)q * zp.nrad + i]);
-    P2 sv[MS];
-    V Lk;
-    Lk.x = T(0); Lk.y = T(0);
+      if (q < np) tq[slot][q] = __ldg(&zp.chi[(long long)q * zp.nrad + i]);
+    lq[slot].x = T(0); lq[slot].y = T(0);
     if (full) {
       if (zp.stab != nullptr) {
 #pragma unroll
         for (int ii = 0; ii < MS; ++ii)
-          if (ii < m) sv[ii] = __ldg(&zp.stab[(long long)ii * zp.nrad + i]);
+          if (ii < m) sq[slot][ii] = __ldg(&zp.stab[(long long)ii * zp.nrad + i]);
       }
-      if (valid) Lk = __ldg(&zp.L[z * zstride + col + b]);
+      if (b < bw) lq[slot] = __ldg(&zp.L[z * zstride + col + b]);
     }
-    V c[MS];
+  };
 #pragma unroll
-    for (int j = 0; j < MS; ++j)
-      if (j < m) c[j] = buf[j * N * B + e];
-    if (full) {
+  for (int s = 0; s < D; ++s) fetch(s, s);
+  if (JOINT) fft2g<N, MS * B, NTHR, false, true, LayCol<N, B>>(buf, tw, tid, act);
+  else
+    for (int s = 0; s < m; ++s) fft2g<N, B, NTHR, false, true, LayCol<N, B>>(buf + s * N * B, tw, tid, act);
+#pragma unroll
+  for (int it = 0; it < NIT; ++it) {
+    const int slot = it % D;
+    const int e = tid + it * NTHR;
+    if (act && e < N * B) {
+      const int b = e % B;
+      const bool valid = b < bw;
+      const T fr = fq[slot];
+      const V Lk = lq[slot];
+      V c[MS];
 #pragma unroll
       for (int j = 0; j < MS; ++j)
-        if (j < m) { c[j].x -= zp.a[j] * Lk.x; c[j].y -= zp.a[j] * Lk.y; }
-    }
-    T xv[NP];
+        if (j < m) c[j] = buf[j * N * B + e];
+      if (full) {
 #pragma unroll
-    for (int q = 0; q < NP; ++q)
-      if (q < np) xv[q] = tv[q].x + tv[q].y * fr;
+        for (int j = 0; j < MS; ++j)
+          if (j < m) { c[j].x -= zp.a[j] * Lk.x; c[j].y -= zp.a[j] * Lk.y; }
+      }
+      T xv[NP];
 #pragma unroll
-    for (int ii = 0; ii < MS; ++ii) {
-      if (ii < m) {
-        V t;
-        t.x = T(0); t.y = T(0);
+      for (int q = 0; q < NP; ++q)
+        if (q < np) xv[q] = tq[slot][q].x + tq[slot][q].y * fr;
 #pragma unroll
-        for (int j = 0; j < MS; ++j) {
-          if (j < m) {
-            const T x = xv[ii >= j ? ii * (ii + 1) / 2 + j : j * (j + 1) / 2 + ii];
-            t.x += x * c[j].x;
-            t.y += x * c[j].y;
+      for (int ii = 0; ii < MS; ++ii) {
+        if (ii < m) {
+          V t;
+          t.x = T(0); t.y = T(0);
+#pragma unroll
+          for (int j = 0; j < MS; ++j) {
+            if (j < m) {
+              const T x = xv[ii >= j ? ii * (ii + 1) / 2 + j : j * (j + 1) / 2 + ii];
+              t.x += x * c[j].x;
+              t.y += x * c[j].y;
+            }
           }
+          if (full) {
+            T bb = zp.bconst[ii];
+            if (zp.stab != nullptr) bb += sq[slot][ii].x + sq[slot][ii].y * fr;
+            t.x -= bb * Lk.x;
+            t.y -= bb * Lk.y;
+          }
+          if (valid) buf[ii * N * B + e] = t;
         }
-        if (full) {
-          T bb = zp.bconst[ii];
-          if (zp.stab != nullptr) bb += sv[ii].x + sv[ii].y * fr;
-          t.x -= bb * Lk.x;
-          t.y -= bb * Lk.y;
-        }
-        if (valid) buf[ii * N * B + e] = t;
       }
     }
+    if (it + D < NIT) fetch(it + D, slot);
   }
   __syncthreads();
   if (JOINT) fft2g<N, MS * B, NTHR, true, true, LayCol<N, B>>(buf, tw, tid, act);
@@ -376,7 +406,8 @@ __device__ __forceinline__ void z_tile(const Geo &g, typename Cx<T>::type *buf, 
 // OZ contraction (+ long-range terms in MODE_F), inverse transform, TMA out.
 // tm: W as {2 Nhp, N1, m N2} scalars, box {2B, 1, N2}.
 template <typename T, int MODE, int N, int B, int MS>
-__global__ void __launch_bounds__(Split<N>::R1 * B) k_z_s(Geo g, const __grid_constant__ CUtensorMap tm,
+__global__ void __launch_bounds__(Split<N>::R1 * B, sizeof(T) == 4 ? 4 : 1) k_z_s(Geo g,
+                                                                                  const __grid_constant__ CUtensorMap tm,
                                                          const typename Cx<T>::type *__restrict__ twg,
                                                          ZParams<T> zp, int *__restrict__ err) {
   using V = typename Cx<T>::type;

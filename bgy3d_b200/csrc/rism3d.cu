@@ -1165,17 +1165,42 @@ bool coarse_graph(rism3d_ctx *c, int k) {
   return ok;
 }
 
-// Solves issued by concurrent host threads (the batch driver) keep the
-// graph-replayed coarse solve: cooperative grids of several streams could
-// each hold part of the GPU while waiting for the rest.
+// Solves issued by concurrent host threads (the batch driver) take the
+// graph-replayed coarse solve.  RISM3D_PK_BATCH=1 gives them the persistent
+// kernel, serialised on the device (below: cooperative grids of several
+// streams could each hold part of the GPU while waiting for the rest).
+// Measured on the 64-solute batch: launches 304 k -> 46 k, but 26.6 -> 21.4
+// solves/s, since one whole-GPU grid at a time stops the streams' coarse
+// solves from overlapping; hence off by default.
 thread_local bool tl_concurrent_solves = false;
+
+bool pk_in_batch() {
+  static const bool on = [] {
+    const char *e = std::getenv("RISM3D_PK_BATCH");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+// One cooperative grid at a time on a device: each persistent launch from a
+// concurrent solve waits (on the device, not the host) for the previous
+// one's completion event, then records its own into the same event.
+struct PkSerial {
+  std::mutex mu;
+  std::map<int, cudaEvent_t> last;  // per device, never destroyed
+};
+PkSerial &pk_serial() {
+  static PkSerial *s = new PkSerial;  // outlives every context
+  return *s;
+}
 
 // The persistent coarse GMRES is used when the coarse grid is a cube with
 // shape-specialised transforms, m <= 3 and k <= 16 (RISM3D_COARSE_PERSIST=0
 // turns it off); its buffers are allocated on first use.
 bool coarse_pk_ready(rism3d_ctx *c, int k) {
-  if (c->pk_grid > 0) return !tl_concurrent_solves;
-  if (c->pk_failed || tl_concurrent_solves) return false;
+  const bool allowed = !tl_concurrent_solves || pk_in_batch();
+  if (c->pk_grid > 0) return allowed;
+  if (c->pk_failed || !allowed) return false;
   const char *env = std::getenv("RISM3D_COARSE_PERSIST");
   rism3d_ctx *cc = c->coarse;
   const Geo &G = cc->g;
@@ -1239,7 +1264,20 @@ bool coarse_pk_run(rism3d_ctx *c, int k) {
   if (trace_ctas && !c->pk_trace_cta)
     c->pk_trace_cta = dalloc<unsigned long long>((size_t)nbar * 2 * c->pk_grid);
   a.trace_cta = trace_ctas ? c->pk_trace_cta : nullptr;
-  const cudaError_t e = coarse_pk_launch(a, cc->g.M, cc->g.N1, c->pk_grid, c->stream);
+  cudaError_t e;
+  if (tl_concurrent_solves) {
+    PkSerial &ps = pk_serial();
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(ps.mu);
+    cudaEvent_t &ev = ps.last[dev];
+    if (!ev) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    else CK(cudaStreamWaitEvent(c->stream, ev, 0));
+    e = coarse_pk_launch(a, cc->g.M, cc->g.N1, c->pk_grid, c->stream);
+    if (e == cudaSuccess) CK(cudaEventRecord(ev, c->stream));
+  } else {
+    e = coarse_pk_launch(a, cc->g.M, cc->g.N1, c->pk_grid, c->stream);
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     c->pk_failed = true;
