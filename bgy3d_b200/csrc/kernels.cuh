@@ -457,25 +457,28 @@ __device__ __forceinline__ double cl0(double r) {     // bgy3d-solutes.c:147-159
 
 // v[i][p] = sum_u eps_iu ljcap0(r/sigma_iu) + q_i q_u/eps0 G cscap0(G r)
 // (field0, bgy3d-solutes.c:343-377); grid point r = i h - L/2.  The pair
-// constants (eps_iu, sigma_iu, q_i q_u / eps0) and the solute positions sit
-// in shared memory ([n][m][3] then [n][3] doubles, kField0MaxPairs pairs at
-// most); the capped Coulomb value of a solute site is evaluated once per
-// point and shared by all solvent sites.  Same terms, same order as the
-// direct form below.
-constexpr int kField0MaxPairs = 1536;
+// constants (eps_iu, 1/sigma_iu, sigma_iu^2, q_i q_u / eps0) and the solute
+// positions sit in shared memory ([n][m][4] then [n][3] doubles,
+// kField0MaxPairs pairs and 384 sites at most).  Per point and solute site
+// one 1/r^2 and one capped Coulomb value serve all solvent sites; per pair
+// r/sigma is a product and (sigma/r)^6 = (sigma^2 / r^2)^3 (a few ulp from
+// the division form below).  The terms sum in the same order.
+constexpr int kField0MaxPairs = 1152;
 static __global__ void __launch_bounds__(256) k_field0_pairs(Geo g, double h0, double h1, double h2, double L0,
                                                              double L1, double L2, const SiteP *__restrict__ solvent,
                                                              int n, const SiteP *__restrict__ solute,
                                                              double *__restrict__ v) {
   extern __shared__ double sp[];
   const int m = g.m;
-  double *sx = sp + 3 * n * m;
+  double *sx = sp + 4 * n * m;
   for (int e = threadIdx.x; e < n * m; e += blockDim.x) {
     const int u = e / m, s = e - u * m;
     const SiteP a = solvent[s], b = solute[u];
-    sp[3 * e] = sqrt(a.epsilon * b.epsilon);
-    sp[3 * e + 1] = 0.5 * (a.sigma + b.sigma);
-    sp[3 * e + 2] = a.charge * b.charge * kEps0Inv;
+    const double sab = 0.5 * (a.sigma + b.sigma);
+    sp[4 * e] = sqrt(a.epsilon * b.epsilon);
+    sp[4 * e + 1] = 1.0 / sab;
+    sp[4 * e + 2] = sab * sab;
+    sp[4 * e + 3] = a.charge * b.charge * kEps0Inv;
   }
   for (int u = threadIdx.x; u < n; u += blockDim.x) {
     sx[3 * u] = solute[u].x;
@@ -494,12 +497,25 @@ static __global__ void __launch_bounds__(256) k_field0_pairs(Geo g, double h0, d
   for (int s = 0; s < kMaxSites; ++s) e[s] = 0.0;
   for (int u = 0; u < n; ++u) {
     const double dx = x - sx[3 * u], dy = y - sx[3 * u + 1], dz = z - sx[3 * u + 2];
-    const double rab = sqrt(dx * dx + dy * dy + dz * dz);
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    const double rab = sqrt(r2);
     const double cs = cscap0(kG * rab);
-    const double *c = sp + 3 * u * m;
+    const double ir2 = 1.0 / r2;  // inf on a site, where every pair takes the capped branch
+    const double *c = sp + 4 * u * m;
 #pragma unroll
-    for (int s = 0; s < kMaxSites; ++s)
-      if (s < m) e[s] += c[3 * s] * ljcap0(rab / c[3 * s + 1]) + c[3 * s + 2] * kG * cs;
+    for (int s = 0; s < kMaxSites; ++s) {
+      if (s < m) {
+        const double xr = rab * c[4 * s + 1];
+        double lj;
+        if (xr >= 0.2) {  // ljcap0's cap radius
+          const double i2 = c[4 * s + 2] * ir2, p6 = i2 * i2 * i2;
+          lj = 4 * p6 * (p6 - 1);
+        } else {
+          lj = ljcap0(xr);
+        }
+        e[s] += c[4 * s] * lj + c[4 * s + 3] * kG * cs;
+      }
+    }
   }
 #pragma unroll
   for (int s = 0; s < kMaxSites; ++s)
