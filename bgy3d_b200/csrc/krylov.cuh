@@ -96,40 +96,63 @@ __global__ void __launch_bounds__(256) k_mdotv(long long nw, const T *__restrict
 
 // w = ws * w - sum_v c_v V_v; part[b] = block b's sum of w^2 (if part).
 // c_v = cf.c[v], times dcoef[v] when dcoef (device-resident coefficients,
-// e.g. dot products reduced on the device) is given.
-template <typename T>
+// e.g. dot products reduced on the device) is given.  NVT (>= nv) bounds the
+// basis vectors held in registers; a thread loads U strided wide elements of
+// every operand before it uses any, so small updates still keep enough bytes
+// in flight to stream at HBM rate.  w is not read when ws == 0 and not
+// written back when the call only measures it (nv == 0, ws == 1).  The
+// arithmetic and the accumulation order are those of the plain strided loop.
+template <typename T, int NVT = kVecMax>
 __global__ void __launch_bounds__(256) k_maxpyv(long long nw, T *__restrict__ w, double ws, int nv, VecSet<T> vs,
                                                Coefs cf, const double *__restrict__ dcoef,
                                                double *__restrict__ part) {
   using VT = typename Wide<T>::type;
   constexpr int WN = Wide<T>::n;
+  constexpr int U = NVT <= 2 ? 4 : (NVT <= 8 ? 2 : 1);
   // the update runs in the basis precision; coefficients converted once
-  T c[kVecMax];
+  T c[NVT];
 #pragma unroll
-  for (int v = 0; v < kVecMax; ++v) c[v] = (T)(dcoef ? (v < nv ? cf.c[v] * dcoef[v] : 0.0) : cf.c[v]);
+  for (int v = 0; v < NVT; ++v) c[v] = (T)(dcoef ? (v < nv ? cf.c[v] * dcoef[v] : 0.0) : cf.c[v]);
   const T wsT = (T)ws;
+  const bool rd = ws != 0.0, wr = !(nv == 0 && ws == 1.0);
+  const long long st = (long long)gridDim.x * blockDim.x;
   double s2 = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += (long long)gridDim.x * blockDim.x) {
-    const VT a = reinterpret_cast<const VT *>(w)[i];
-    const T *ar = reinterpret_cast<const T *>(&a);
-    VT o;
-    T *r = reinterpret_cast<T *>(&o);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += U * st) {
+    VT a[U], b[U][NVT];
 #pragma unroll
-    for (int q = 0; q < WN; ++q) r[q] = ws == 0.0 ? T(0) : wsT * ar[q];
+    for (int u = 0; u < U; ++u) {
+      const long long iu = i + u * st;
+      if (iu < nw) {
+        if (rd) a[u] = reinterpret_cast<const VT *>(w)[iu];
 #pragma unroll
-    for (int v = 0; v < kVecMax; ++v) {
-      if (v < nv) {
-        const VT b = reinterpret_cast<const VT *>(vs.p[v])[i];
-        const T *br = reinterpret_cast<const T *>(&b);
-#pragma unroll
-        for (int q = 0; q < WN; ++q) r[q] -= c[v] * br[q];
+        for (int v = 0; v < NVT; ++v)
+          if (v < nv) b[u][v] = reinterpret_cast<const VT *>(vs.p[v])[iu];
       }
     }
-    T sq = T(0);
 #pragma unroll
-    for (int q = 0; q < WN; ++q) sq += r[q] * r[q];
-    s2 += (double)sq;
-    reinterpret_cast<VT *>(w)[i] = o;
+    for (int u = 0; u < U; ++u) {
+      const long long iu = i + u * st;
+      if (iu < nw) {
+        const T *ar = reinterpret_cast<const T *>(&a[u]);
+        VT o;
+        T *r = reinterpret_cast<T *>(&o);
+#pragma unroll
+        for (int q = 0; q < WN; ++q) r[q] = rd ? wsT * ar[q] : T(0);
+#pragma unroll
+        for (int v = 0; v < NVT; ++v) {
+          if (v < nv) {
+            const T *br = reinterpret_cast<const T *>(&b[u][v]);
+#pragma unroll
+            for (int q = 0; q < WN; ++q) r[q] -= c[v] * br[q];
+          }
+        }
+        T sq = T(0);
+#pragma unroll
+        for (int q = 0; q < WN; ++q) sq += r[q] * r[q];
+        s2 += (double)sq;
+        if (wr) reinterpret_cast<VT *>(w)[iu] = o;
+      }
+    }
   }
   if (part) {
     for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
@@ -346,6 +369,17 @@ void launch_mdotv(unsigned grid, cudaStream_t st, long long nw, const T *w, int 
   else if (nv <= 8) k_mdotv<T, 8><<<grid, 256, 0, st>>>(nw, w, nv, vs, part);
   else if (nv <= 16) k_mdotv<T, 16><<<grid, 256, 0, st>>>(nw, w, nv, vs, part);
   else k_mdotv<T, kVecMax><<<grid, 256, 0, st>>>(nw, w, nv, vs, part);
+}
+// Launch of the update with the smallest basis bound NVT >= nv.
+template <typename T>
+void launch_maxpyv(unsigned grid, cudaStream_t st, long long nw, T *w, double ws, int nv, const VecSet<T> &vs,
+                   const Coefs &cf, const double *dcoef, double *part) {
+  if (nv <= 1) k_maxpyv<T, 1><<<grid, 256, 0, st>>>(nw, w, ws, nv, vs, cf, dcoef, part);
+  else if (nv <= 2) k_maxpyv<T, 2><<<grid, 256, 0, st>>>(nw, w, ws, nv, vs, cf, dcoef, part);
+  else if (nv <= 4) k_maxpyv<T, 4><<<grid, 256, 0, st>>>(nw, w, ws, nv, vs, cf, dcoef, part);
+  else if (nv <= 8) k_maxpyv<T, 8><<<grid, 256, 0, st>>>(nw, w, ws, nv, vs, cf, dcoef, part);
+  else if (nv <= 16) k_maxpyv<T, 16><<<grid, 256, 0, st>>>(nw, w, ws, nv, vs, cf, dcoef, part);
+  else k_maxpyv<T, kVecMax><<<grid, 256, 0, st>>>(nw, w, ws, nv, vs, cf, dcoef, part);
 }
 template <typename T>
 void launch_mdot_red(unsigned grid, cudaStream_t st, long long nw, const T *w, int nv, const VecSet<T> &vs,

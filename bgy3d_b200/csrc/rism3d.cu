@@ -711,8 +711,8 @@ double maxpy(rism3d_ctx *c, T *w, double ws, const std::vector<VecRef<T>> &V, co
       cf.c[i] = i < k ? coef[base + i] * V[base + i].s : 0.0;
     }
     const bool last = base + kVecMax >= nv;
-    k_maxpyv<T><<<G, 256, 0, c->stream>>>(nw, w, base == 0 ? ws : 1.0, std::max(k, 0), vs, cf, nullptr,
-                                           (last && want_norm) ? c->dpart : nullptr);
+    launch_maxpyv<T>(G, c->stream, nw, w, base == 0 ? ws : 1.0, std::max(k, 0), vs, cf, nullptr,
+                     (last && want_norm) ? c->dpart : nullptr);
     CKL();
   }
   if (!want_norm) return 0.0;
@@ -745,7 +745,7 @@ double gs_step(rism3d_ctx *c, T *w, const std::vector<VecRef<T>> &V, std::vector
   CKL();
   k_colsum<<<1, kVecMax * 8, 0, c->stream>>>(G, kVecMax, nv, c->dpart, c->dres);
   CKL();
-  k_maxpyv<T><<<G, 256, 0, c->stream>>>(nw, w, 1.0, nv, vs, cf, c->dres, c->dpart);
+  launch_maxpyv<T>(G, c->stream, nw, w, 1.0, nv, vs, cf, c->dres, c->dpart);
   CKL();
   k_colsum<<<1, kVecMax * 8, 0, c->stream>>>(G, 1, 1, c->dpart, c->dres + kVecMax);
   CKL();
@@ -1090,7 +1090,7 @@ void coarse_solve_dev(rism3d_ctx *c, int k) {
   double *H = c->cg_H, *nrm = c->cg_aux, *beta = c->cg_aux + 1, *y = c->cg_aux + 2;
   Coefs one{}, mone{};
   for (int i = 0; i < kVecMax; ++i) one.c[i] = 1.0, mone.c[i] = -1.0;
-  k_maxpyv<float><<<G, 256, 0, st>>>(nw, B[0], 1.0, 0, VecSet<float>{}, one, nullptr, cc->dpart);
+  launch_maxpyv<float>(G, st, nw, B[0], 1.0, 0, VecSet<float>{}, one, nullptr, cc->dpart);
   k_colsum<<<1, kVecMax * 8, 0, st>>>(G, 1, 1, cc->dpart, nrm);  // |r|^2
   k_scale_norm<float><<<gv, 256, 0, st>>>(cc->nvec, B[0], nrm, beta);
   CKL();
@@ -1108,7 +1108,7 @@ void coarse_solve_dev(rism3d_ctx *c, int k) {
   k_arnoldi_lsq<<<1, 1, 0, st>>>(k, H, beta, y);
   VecSet<float> vs{};
   for (int i = 0; i < kVecMax; ++i) vs.p[i] = B[i < k ? i : 0];
-  k_maxpyv<float><<<G, 256, 0, st>>>(nw, c->tc_y, 0.0, k, vs, mone, y, nullptr);
+  launch_maxpyv<float>(G, st, nw, c->tc_y, 0.0, k, vs, mone, y, nullptr);
   CKL();
 }
 
