@@ -93,7 +93,7 @@ EXPORTS = [
     "rism3d_jacobian_t1", "rism3d_iterate_t1_f32", "rism3d_jacobian_t1_f32",
     "rism3d_solve", "rism3d_observables", "rism3d_get_field", "rism3d_last_error",
     "rism3d_profile", "rism1d_solvent_chi", "rism3d_jacobian_apply_noalloc",
-    "rism3d_precondition", "rism3d_coarse_grid", "rism3d_coarse_driver", "rism3d_solve_batch",
+    "rism3d_precondition", "rism3d_precondition_f32", "rism3d_coarse_grid", "rism3d_coarse_driver", "rism3d_solve_batch",
     "rism3d_solute_grad", "rism3d_gradient", "rism3d_jacobian_transpose_t1", "rism3d_ctx_set_solute",
     "rism3d_response", "rism3d_solvent_solve", "rism3d_solvent_ctx_create", "rism3d_ctx_create_chi3",
     "rism3d_solute_solve_chi3", "rism3d_info", "rism3d_moments", "rism3d_tile_shapes",
@@ -144,6 +144,8 @@ def lib():
     L.rism3d_jacobian_apply_noalloc.restype = I
     L.rism3d_precondition.argtypes = [V, V, V, V]
     L.rism3d_precondition.restype = I
+    L.rism3d_precondition_f32.argtypes = [V, V, V, V]
+    L.rism3d_precondition_f32.restype = I
     L.rism3d_coarse_grid.argtypes = [V, P(I)]
     L.rism3d_coarse_grid.restype = I
     L.rism3d_coarse_driver.argtypes = [V]

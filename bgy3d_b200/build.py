@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librism3d.so")
-SOURCES = ["rism3d.cu", "twogrid_fx2.cu", "twogrid_yz.cu", "coarse_pk.cu", "rism1d.cpp", "noalloc.cu"]
+SOURCES = ["rism3d.cu", "twogrid_fx2.cu", "twogrid_yz.cu", "twogrid_tc.cu", "coarse_pk.cu", "rism1d.cpp", "noalloc.cu"]
 HEADERS = ["fft_core.cuh", "kernels.cuh", "fft_static.cuh", "kernels_static.cuh", "krylov.cuh", "twogrid.cuh",
            "twogrid_fft.cuh", "grad.cuh", "solvent.cuh", "info.cuh", "coarse_pk.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

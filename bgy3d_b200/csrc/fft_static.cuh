@@ -177,6 +177,9 @@ __device__ __forceinline__ void fft2(V *buf, const V *tw) {
 }
 
 // ------------------------------------------------------------- TMA + mbarrier
+// d_err code of a timed-out wait in the tensor-core grid transfers
+// (the passes record their pass number, the coarse solve kPkErr).
+constexpr int kTcErr = 6;
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }

@@ -53,6 +53,12 @@ bool fx2_restrict(int M, int MC, long long rows, const T *in, float s, const flo
 template <typename T>
 bool fx2_prolong(int M, int MC, long long rows, const float *y, const float2 *post, const float2 *tw,
                  const float2 *postc, const float2 *twc, const T *r, double s, T *out, cudaStream_t st);
+// twogrid_tc.cu: the x transfers of FP32 data on the tensor cores
+bool tc_x_has(int n0, int nc);
+bool tc_restrict_x(long long rows, int n0, int nc, const float *in, float s, const float *R, float *out, int *err,
+                   cudaStream_t st);
+bool tc_prolong_x(long long rows, int n0, int nc, const float *y, const float *P, const float *r, float s, float *out,
+                  int *err, cudaStream_t st);
 }  // namespace rism
 
 namespace {
@@ -577,8 +583,9 @@ void reduce_norms(rism3d_ctx *c, int nblk, double *resid) {
   CK(cudaMemcpyAsync(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (err) {
-    g_last_error = err == kPkErr ? std::string("a bounded grid-barrier wait timed out in the coarse solve")
-                                 : "a bounded TMA/mbarrier wait timed out in pass " + std::to_string(err);
+    g_last_error = err == kPkErr   ? std::string("a bounded grid-barrier wait timed out in the coarse solve")
+                   : err == kTcErr ? std::string("a bounded mbarrier wait timed out in a tensor-core grid transfer")
+                                   : "a bounded TMA/mbarrier wait timed out in pass " + std::to_string(err);
     throw CudaFail{RISM3D_ERR_CUDA};
   }
   double amax = 0.0, s2 = 0.0;
@@ -1036,11 +1043,28 @@ template <typename T> bool fx_prolong(rism3d_ctx *c, long long rows, const T *r,
   return true;
 }
 
+// The x transfers of FP32 data on the tensor cores (twogrid_tc.cu) where the
+// (fine, coarse) pair has a kernel; RISM3D_TC_TRANSFERS=0, or either dense
+// switch (RISM3D_DENSE_TRANSFERS=1/2), selects the FFT or dense forms.
+bool tc_usable(const rism3d_ctx *c) {
+  const char *off = std::getenv("RISM3D_TC_TRANSFERS");
+  const char *dense = std::getenv("RISM3D_DENSE_TRANSFERS");
+  if ((off && off[0] == '0') || (dense && (dense[0] == '1' || dense[0] == '2'))) return false;
+  return c->coarse && c->tR[0] && c->tP[0] && rism::tc_x_has(c->g.N0, c->Nc[0]);
+}
+
 // out (coarse [m][Nc2][Nc1][Nc0]) = R (s in), in fine [m][N2][N1][N0].
 template <typename T> void tg_restrict(rism3d_ctx *c, const T *in, double s, float *out) {
   const Geo &G = c->g;
   const long long rows = (long long)c->m * G.N2 * G.N1;
-  if (!fx_restrict<T>(c, rows, in, s)) {
+  bool tc = false;
+  if constexpr (sizeof(T) == 4) {
+    if (tc_usable(c)) {
+      tc = rism::tc_restrict_x(rows, G.N0, c->Nc[0], in, (float)s, c->tR[0], c->tA, c->d_err, c->stream);
+      CKL();
+    }
+  }
+  if (!tc && !fx_restrict<T>(c, rows, in, s)) {
     dim3 gx((unsigned)((rows + tg::kRxRows - 1) / tg::kRxRows),
             (unsigned)((c->Nc[0] + tg::kRxCols - 1) / tg::kRxCols));
     tg::k_restrict_x<T><<<gx, tg::kRxThreads, 0, c->stream>>>(rows, G.N0, c->Nc[0], in, (float)s, c->tRt[0], c->tA);
@@ -1056,7 +1080,14 @@ template <typename T> void tg_prolong(rism3d_ctx *c, const float *yc, const T *r
   transfer_axis(c, 2, c->m, c->Nc[2], G.N2, c->Nc[1] * c->Nc[0], yc, c->tP[2], c->tB);
   transfer_axis(c, 1, c->m * G.N2, c->Nc[1], G.N1, c->Nc[0], c->tB, c->tP[1], c->tA);
   const long long rows = (long long)c->m * G.N2 * G.N1;
-  if (!fx_prolong<T>(c, rows, r, s, out)) {
+  bool tc = false;
+  if constexpr (sizeof(T) == 4) {
+    if (tc_usable(c)) {
+      tc = rism::tc_prolong_x(rows, G.N0, c->Nc[0], c->tA, c->tP[0], r, (float)s, out, c->d_err, c->stream);
+      CKL();
+    }
+  }
+  if (!tc && !fx_prolong<T>(c, rows, r, s, out)) {
     dim3 gx((unsigned)((rows + tg::kPxRows - 1) / tg::kPxRows), (unsigned)((G.N0 + tg::kPxCols - 1) / tg::kPxCols));
     tg::k_prolong_x<T, T><<<gx, tg::kPxThreads, 0, c->stream>>>(rows, G.N0, c->Nc[0], c->tA, c->tPt[0], r, s, out);
     CKL();
@@ -3693,6 +3724,19 @@ int rism3d_precondition(rism3d_ctx *ctx, const double *T, const double *v, doubl
     closure_slope<double, double>(ctx, T, d);
     tg_prepare<double>(ctx, d);
     tg_apply<double>(ctx, v, 1.0, z);
+    CK(cudaStreamSynchronize(ctx->stream));
+    return (int)RISM3D_OK;
+  });
+}
+
+int rism3d_precondition_f32(rism3d_ctx *ctx, const float *T, const float *v, float *z) {
+  if (!ctx || !T || !v || !z) return RISM3D_ERR_ARG;
+  if (!ctx->coarse) return RISM3D_ERR_UNSUPPORTED;
+  return guard([&] {
+    float *d = slopebuf<float>(ctx);
+    closure_slope<float, float>(ctx, T, d);
+    tg_prepare<float>(ctx, d);
+    tg_apply<float>(ctx, v, 1.0, z);
     CK(cudaStreamSynchronize(ctx->stream));
     return (int)RISM3D_OK;
   });

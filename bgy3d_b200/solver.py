@@ -424,9 +424,15 @@ class RismContext:
         return {2: "persistent", 1: "graph", 0: "host"}.get(r)
 
     def precondition(self, T, v, out=None):
-        """Two-grid preconditioner at state T: M^-1 v (FP64 device tensors)."""
+        """Two-grid preconditioner at state T: M^-1 v.  FP64 device tensors,
+        or FP32 ones for the mixed solve's FP32 form of it."""
         t = self._torch
         out = t.empty_like(v) if out is None else out
+        if v.dtype == t.float32:
+            _abi.check(_abi.lib().rism3d_precondition_f32(self._h, self._check_vec(T, t.float32),
+                                                          self._check_vec(v, t.float32),
+                                                          self._check_vec(out, t.float32)), "precondition_f32")
+            return out
         _abi.check(_abi.lib().rism3d_precondition(self._h, self._check_vec(T, t.float64),
                                                   self._check_vec(v, t.float64),
                                                   self._check_vec(out, t.float64)), "precondition")

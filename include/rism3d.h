@@ -275,6 +275,11 @@ const char *rism3d_last_error(void);
    RISM3D_ERR_UNSUPPORTED when the context has no coarse grid. */
 int rism3d_precondition(rism3d_ctx *ctx, const double *T, const double *v, double *z);
 
+/* The same preconditioner in FP32, as the mixed-precision solve applies it
+   (FP32 device pointers [m][N2][N1][N0]); its x-axis grid transfers run on
+   the tensor cores where the (fine, coarse) pair has a kernel. */
+int rism3d_precondition_f32(rism3d_ctx *ctx, const float *T, const float *v, float *z);
+
 /* Rebinds the context to another solute of the same solvent and grid (a
    new geometry, charges or LJ parameters): recomputes the solute's
    short-range field and long-range term only, keeping every buffer, the

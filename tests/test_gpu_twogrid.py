@@ -184,6 +184,37 @@ def test_fft_transfers_match_dense_long_rows(fixture_loader, N, L, monkeypatch):
         assert np.max(np.abs(z - out[2])) < 1e-4 * np.max(np.abs(out[2]))
 
 
+@pytest.mark.parametrize("N", [(256, 48, 48), (192, 48, 48), (128, 48, 48)])
+def test_tensor_core_transfers(fixture_loader, N, monkeypatch):
+    """x rows of 256, 192 and 128 points onto a 64-point coarse axis (a 48 A
+    box): the FP32 preconditioner with the x transfers on the tensor cores
+    (TF32 products in three terms, hi.hi + hi.lo + lo.hi) equals the one
+    with the FFT x transfers (RISM3D_TC_TRANSFERS=0) to FP32 accuracy, and
+    the FP64 preconditioner with the dense transfer tiles to the 1e-4 of the
+    other preconditioner tests (the coarse solve is FP32 in both)."""
+    meta, arr = fixture_loader("synth6_kh_n32")
+    s = settings_of(meta, N=list(N), L=[24.0, 4.5, 4.5])
+    rng = np.random.default_rng(12)
+    out = {}
+    for tc in ("1", "0"):
+        monkeypatch.setenv("RISM3D_TC_TRANSFERS", tc)
+        ctx = RismContext(meta["solute"], meta["solvent"], s, arr["chi"])
+        assert ctx.coarse_grid()[0] == 64
+        if not out:
+            T = 0.3 * rng.standard_normal(ctx.shape)
+            v = rng.standard_normal(ctx.shape)
+        out[tc] = ctx.precondition(to_dev(T, torch.float32), to_dev(v, torch.float32)).double().cpu().numpy()
+        ctx.close()
+    monkeypatch.setenv("RISM3D_DENSE_TRANSFERS", "1")
+    ctx = RismContext(meta["solute"], meta["solvent"], s, arr["chi"])
+    ref = ctx.precondition(to_dev(T), to_dev(v)).cpu().numpy()
+    ctx.close()
+    scale = np.max(np.abs(ref))
+    assert np.max(np.abs(out["1"] - out["0"])) < 2e-5 * scale
+    assert np.max(np.abs(out["1"] - ref)) < 1e-4 * scale
+    assert np.max(np.abs(out["0"] - ref)) < 1e-4 * scale
+
+
 @pytest.mark.parametrize("n", [96, 128])
 def test_persistent_coarse_solve(fixture_loader, n, monkeypatch):
     """The coarse GMRES as one persistent cooperative kernel (coarse grids
