@@ -112,6 +112,37 @@ template <> struct Vec2<float> { using type = float2; };
 // ------------------------------------------------------------- reductions
 struct NormPartial { double amax, sum2; };
 
+// out[0] = the largest amax (a NaN anywhere gives NaN), out[1] = the sum of
+// sum2, out[2] = *err: the block partials of one residual reduced on the
+// device in one fixed order (strided per thread, then a pairwise tree), so
+// that three doubles, not the partials, cross to the host.
+__device__ __forceinline__ double amax_merge(double a, double x) { return (a != a) ? a : ((x > a || x != x) ? x : a); }
+__global__ static void __launch_bounds__(1024) k_norm_final(int nblk, const NormPartial *__restrict__ part,
+                                                            const int *__restrict__ err, double *__restrict__ out) {
+  __shared__ double sa[1024], ss[1024];
+  const int t = threadIdx.x;
+  double a = 0.0, s = 0.0;
+  for (int b = t; b < nblk; b += 1024) {
+    a = amax_merge(a, part[b].amax);
+    s += part[b].sum2;
+  }
+  sa[t] = a;
+  ss[t] = s;
+  __syncthreads();
+  for (int st = 512; st > 0; st >>= 1) {
+    if (t < st) {
+      sa[t] = amax_merge(sa[t], sa[t + st]);
+      ss[t] += ss[t + st];
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    out[0] = sa[0];
+    out[1] = ss[0];
+    out[2] = (double)*err;
+  }
+}
+
 __device__ __forceinline__ void block_norms(double amax, double sum2, NormPartial *out) {
   for (int o = 16; o > 0; o >>= 1) {
     amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));

@@ -235,7 +235,6 @@ struct rism3d_ctx {
   double *d_charge = nullptr;
 
   NormPartial *npart = nullptr;
-  std::vector<NormPartial> h_npart;
   double *dpart = nullptr;       // [red_blocks][kVecMax] reduction partials
   double *dres = nullptr;        // [kVecMax * 2] reduced coefficients (device)
   std::vector<double> h_dpart;
@@ -576,26 +575,21 @@ template <typename T, int MODE> void launch_z(rism3d_ctx *c) {
 }
 
 void reduce_norms(rism3d_ctx *c, int nblk, double *resid) {
-  c->h_npart.resize(nblk);
-  CK(cudaMemcpyAsync(c->h_npart.data(), c->npart, sizeof(NormPartial) * nblk, cudaMemcpyDeviceToHost,
-                     c->stream));
-  int err = 0;
-  CK(cudaMemcpyAsync(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  double *dout = c->dres + 2 * kVecMax;
+  k_norm_final<<<1, 1024, 0, c->stream>>>(nblk, c->npart, c->d_err, dout);
+  CKL();
+  double *h = pinned_scratch();
+  CK(cudaMemcpyAsync(h, dout, sizeof(double) * 3, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  const int err = (int)h[2];
   if (err) {
     g_last_error = err == kPkErr   ? std::string("a bounded grid-barrier wait timed out in the coarse solve")
                    : err == kTcErr ? std::string("a bounded mbarrier wait timed out in a tensor-core grid transfer")
                                    : "a bounded TMA/mbarrier wait timed out in pass " + std::to_string(err);
     throw CudaFail{RISM3D_ERR_CUDA};
   }
-  double amax = 0.0, s2 = 0.0;
-  for (int i = 0; i < nblk; ++i) {
-    const double a = c->h_npart[i].amax;
-    amax = (a > amax || a != a) ? a : amax;
-    s2 += c->h_npart[i].sum2;
-  }
-  resid[0] = amax;
-  resid[1] = std::sqrt(s2);
+  resid[0] = h[0];
+  resid[1] = std::sqrt(h[1]);
 }
 
 // The five passes of one residual (MODE_F: A = t, Bv = v, p = beta) or
