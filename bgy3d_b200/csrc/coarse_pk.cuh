@@ -166,13 +166,21 @@ template <int M> __host__ __device__ constexpr int pk_rx() {
 // of each).
 template <int CNT> __host__ __device__ constexpr int pk_group() { return CNT <= 2 ? 4 : 2; }
 
+// The column tile of the plane phases: [N][M + 2] complex (y, kx), the row
+// stride of W (Nhp = M + 2 for the even M here), after the row tile.
+template <int M> __host__ __device__ constexpr int pk_ncp() { return M + 2; }
+
 // XF: V_j -= sum_{i<nu} cf_i V_i (nu = 0: no update) with |V_j|^2 into nrm2;
-// then, if fft, c'_H V_j and the r2c along x into W.
-template <int M>
+// then, if fft, c'_H V_j and the r2c along x into W.  PLANE (RX = N, the
+// rows of one (site, z) plane per item): the spectrum goes into the column
+// tile, is transformed along y as well, and the plane is stored to W whole.
+template <int M, int RX = pk_rx<M>(), bool PLANE = false, int N = RX>
 __device__ __forceinline__ void pk_xf(const PkArgs &a, float *const *V, int j, int nu, const float *cf, bool fft,
-                                      float2 *buf, const float2 *tw, double &nrm2) {
-  constexpr int RX = pk_rx<M>();
+                                      float2 *buf, const float2 *tw, const float2 *twy, double &nrm2) {
+  static_assert(!PLANE || RX == N, "a plane item holds the N rows of one (site, z) plane");
   using Lay = LayRow<M, PkSplit<M>::R2>;
+  constexpr int NCP = pk_ncp<M>();
+  float2 *T = buf + RX * Lay::RS;  // PLANE: the column tile
   constexpr int PER_ROW = M / 2;  // float4 per row (two complex values)
   constexpr int CNT = (RX * PER_ROW + kPkThreads - 1) / kPkThreads;
   constexpr int H = M / 2 + 1;
@@ -258,22 +266,32 @@ __device__ __forceinline__ void pk_xf(const PkArgs &a, float *const *V, int j, i
       O.x = (zk.y + zm.y) * 0.5f;
       O.y = -(zk.x - zm.x) * 0.5f;
       const float2 wO = cmul(a.post[kk], O);
-      float2 *row_out = a.W + (long long)grow * a.g.Nhp;
+      float2 *row_out = PLANE ? T + row * NCP : a.W + (long long)grow * a.g.Nhp;
       row_out[kk] = cadd(E, wO);
       if (M - kk != kk) row_out[M - kk] = cconj(csub(E, wO));
     }
     __syncthreads();  // buf is refilled by the next item
+    if constexpr (PLANE) {
+      fft2g<N, M + 1, kPkThreads, false, true, LayCol<N, NCP>>(T, twy, tid, true);
+      float4 *dst = reinterpret_cast<float4 *>(a.W + (long long)item * N * NCP);
+      const float4 *src = reinterpret_cast<const float4 *>(T);
+      for (int e = tid; e < N * NCP / 2; e += kPkThreads) dst[e] = src[e];
+      __syncthreads();  // T is refilled by the next item
+    }
   }
 }
 
 // XI: V_{j+1} = sc X - sub V_j (X the c2r of W along x), with the dots
 // <V_i, V_{j+1}>, i <= j, summed per warp into sdot[i][warp] (shared, zeroed
-// by the caller).
-template <int M>
+// by the caller).  PLANE: the item's plane of W is loaded whole into the
+// column tile and transformed back along y first.
+template <int M, int RX = pk_rx<M>(), bool PLANE = false, int N = RX>
 __device__ __forceinline__ void pk_xi(const PkArgs &a, float *const *V, int j, float sc, float sub, float2 *buf,
-                                      const float2 *tw, double (*sdot)[kPkThreads / 32]) {
-  constexpr int RX = pk_rx<M>();
+                                      const float2 *tw, const float2 *twy, double (*sdot)[kPkThreads / 32]) {
+  static_assert(!PLANE || RX == N, "a plane item holds the N rows of one (site, z) plane");
   using Lay = LayRow<M, PkSplit<M>::R2>;
+  constexpr int NCP = pk_ncp<M>();
+  float2 *T = buf + RX * Lay::RS;  // PLANE: the column tile
   constexpr int PER_ROW = M / 2;
   constexpr int CNT = (RX * PER_ROW + kPkThreads - 1) / kPkThreads;
   constexpr int GV = pk_group<CNT>();
@@ -295,12 +313,19 @@ __device__ __forceinline__ void pk_xi(const PkArgs &a, float *const *V, int j, f
       if (e < RX * PER_ROW && row0 + row < rows_total)
         rin[it] = *reinterpret_cast<const float4 *>(vin + (long long)(row0 + row) * a.g.N0 + 2 * jj);
     }
+    if constexpr (PLANE) {
+      const float4 *src = reinterpret_cast<const float4 *>(a.W + (long long)item * N * NCP);
+      float4 *dst = reinterpret_cast<float4 *>(T);
+      for (int e = tid; e < N * NCP / 2; e += kPkThreads) dst[e] = src[e];
+      __syncthreads();
+      fft2g<N, M + 1, kPkThreads, true, true, LayCol<N, NCP>>(T, twy, tid, true);
+    }
     for (int e = tid; e < RX * H; e += kPkThreads) {
       const int row = e / H, kk = e % H;
       const int grow = row0 + row;
       float2 zk = make_float2(0.f, 0.f), zm = make_float2(0.f, 0.f);
       if (grow < rows_total) {
-        const float2 *row_in = a.W + (long long)grow * a.g.Nhp;
+        const float2 *row_in = PLANE ? T + row * NCP : a.W + (long long)grow * a.g.Nhp;
         float2 xk = row_in[kk];
         float2 xm = row_in[M - kk];
         if (kk == 0) { xk.y = 0.f; xm.y = 0.f; }  // c2r reads only Re X_0, Re X_{N0/2}
@@ -478,17 +503,25 @@ __device__ __forceinline__ void pk_lsq(int k, double *H, double beta, double *y,
 }
 
 // Shared memory of the phases (dynamic part): the three twiddle tables and
-// the largest work tile.
-template <int M, int N> __host__ __device__ constexpr size_t pk_smem() {
-  constexpr size_t xs = (size_t)pk_rx<M>() * LayRow<M, PkSplit<M>::R2>::RS;
-  constexpr size_t ys = (size_t)(kPkThreads / (Split<N>::R1 * 16)) * N * 16;
+// the largest work tile (PLANE: a plane's row tile and its column tile).
+template <int M, int N, bool PLANE = false> __host__ __device__ constexpr size_t pk_smem() {
+  constexpr size_t xs = PLANE ? (size_t)N * (LayRow<M, PkSplit<M>::R2>::RS + pk_ncp<M>())
+                              : (size_t)pk_rx<M>() * LayRow<M, PkSplit<M>::R2>::RS;
+  constexpr size_t ys = PLANE ? 0 : (size_t)(kPkThreads / (Split<N>::R1 * 16)) * N * 16;
   constexpr size_t zs = (size_t)(kPkThreads / (Split<N>::R1 * kPkBz * 3)) * 3 * N * kPkBz;
   constexpr size_t tile = xs > ys ? (xs > zs ? xs : zs) : (ys > zs ? ys : zs);
   return sizeof(float2) * (M + 2 * N + tile);
 }
 
-template <int M, int N>
+// Grid barriers of one GMRES step: XF Y Z YI XI, or XY Z YXI with PLANE.
+template <bool PLANE> __host__ __device__ constexpr int pk_phases() { return PLANE ? 3 : 5; }
+
+// PLANE: every CTA owns whole (site, z) planes in the x phases, so that the
+// y transforms ride in them (XY: update, c'_H, r2c along x, forward y; YXI:
+// inverse y, c2r along x, dots) and a step has three grid barriers, not five.
+template <int M, int N, bool PLANE = false>
 __global__ void __launch_bounds__(kPkThreads, 2) k_coarse_gmres(PkArgs a) {
+  constexpr int RXP = PLANE ? N : pk_rx<M>();
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float2 *twx = reinterpret_cast<float2 *>(smem_raw);
   float2 *twy = twx + M;
@@ -541,7 +574,7 @@ __global__ void __launch_bounds__(kPkThreads, 2) k_coarse_gmres(PkArgs a) {
       }
       __syncthreads();
     }
-    pk_xf<M>(a, sV, j, j, sC, j < k, tile, twx, nrm2);
+    pk_xf<M, RXP, PLANE, N>(a, sV, j, j, sC, j < k, tile, twx, twy, nrm2);
     if (j > 0) pk_block_sum(nrm2, a.pnrm + (j & 1) * gridDim.x);
     if (!grid_sync(a.bar, ++gen, a.err, a.trace, a.trace_cta)) return;
     if (j > 0) {
@@ -553,19 +586,23 @@ __global__ void __launch_bounds__(kPkThreads, 2) k_coarse_gmres(PkArgs a) {
       __syncthreads();
     }
     if (j == k) break;
-    pk_y<N, false>(a, tile, twy);
-    if (!grid_sync(a.bar, ++gen, a.err, a.trace, a.trace_cta)) return;
+    if constexpr (!PLANE) {
+      pk_y<N, false>(a, tile, twy);
+      if (!grid_sync(a.bar, ++gen, a.err, a.trace, a.trace_cta)) return;
+    }
     pk_z<N>(a, tile, twz);
     if (!grid_sync(a.bar, ++gen, a.err, a.trace, a.trace_cta)) return;
-    pk_y<N, true>(a, tile, twy);
-    if (!grid_sync(a.bar, ++gen, a.err, a.trace, a.trace_cta)) return;
+    if constexpr (!PLANE) {
+      pk_y<N, true>(a, tile, twy);
+      if (!grid_sync(a.bar, ++gen, a.err, a.trace, a.trace_cta)) return;
+    }
     // V_{j+1} = J (V_j / s_j) = (X / N - V_j) / s_j
     const double sj = sS[j];
     const float inv = sj > 0.0 ? (float)(1.0 / sj) : 0.f;
     __shared__ double sdot[kPkMaxSteps][kPkThreads / 32];
     for (int q = tid; q < kPkMaxSteps * (kPkThreads / 32); q += kPkThreads) (&sdot[0][0])[q] = 0.0;
     __syncthreads();
-    pk_xi<M>(a, sV, j, scale * inv, inv, tile, twx, sdot);
+    pk_xi<M, RXP, PLANE, N>(a, sV, j, scale * inv, inv, tile, twx, twy, sdot);
     if (tid <= j) {
       double t = 0.0;
       for (int w = 0; w < kPkThreads / 32; ++w) t += sdot[tid][w];

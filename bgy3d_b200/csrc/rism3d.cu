@@ -46,6 +46,7 @@ bool yz_fft_transfer(int outer, int n_in, int n_out, int inner, const float *in,
                      const float2 *two, float *out, cudaStream_t st);
 // coarse_pk.cu: the persistent cooperative coarse GMRES
 int coarse_pk_grid(int M, int N, int per_sm);
+int coarse_pk_phases(int M, int N);
 cudaError_t coarse_pk_launch(const PkArgs &a, int M, int N, int grid, cudaStream_t st);
 template <typename T>
 bool fx2_restrict(int M, int MC, long long rows, const T *in, float s, const float2 *post, const float2 *tw,
@@ -1281,10 +1282,11 @@ bool coarse_pk_run(rism3d_ctx *c, int k) {
     return t ? std::atoi(t) : 0;
   }();
   const bool trace = trace_level > 0, trace_steps = trace_level > 1;
-  const int nts = 5 * k + 4;
+  const int P = coarse_pk_phases(cc->g.M, cc->g.N1);  // grid barriers per step
+  const int nts = P * k + 4;
   if (trace && !c->pk_trace) c->pk_trace = dalloc<unsigned long long>((size_t)nts);
   a.trace = trace ? c->pk_trace : nullptr;
-  const int nbar = 5 * k + 2;
+  const int nbar = P * k + 2;
   const bool trace_ctas = trace_level > 2;
   if (trace_ctas && !c->pk_trace_cta)
     c->pk_trace_cta = dalloc<unsigned long long>((size_t)nbar * 2 * c->pk_grid);
@@ -1314,17 +1316,18 @@ bool coarse_pk_run(rism3d_ctx *c, int k) {
     CK(cudaMemcpyAsync(ts.data(), c->pk_trace, sizeof(unsigned long long) * nts, cudaMemcpyDeviceToHost,
                        c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    // phases: P0, then per step XF Y Z YI XI, then the last update, then the sum
+    // phases: P0, then per step XF Y Z YI XI (XY Z YXI in the plane form),
+    // then the last update, then the sum
+    const char *names5[5] = {"XF", "Y", "Z", "YI", "XI"}, *names3[3] = {"XY", "Z", "YXI"};
+    const char *const *names = P == 3 ? names3 : names5;
     double ph[7] = {0, 0, 0, 0, 0, 0, 0};
     ph[0] = (double)(ts[1] - ts[0]);
     for (int j = 0; j < k; ++j)
-      for (int p = 0; p < 5; ++p) ph[1 + p] += (double)(ts[2 + 5 * j + p] - ts[1 + 5 * j + p]);
-    ph[6] = (double)(ts[5 * k + 3] - ts[5 * k + 1]);
-    std::fprintf(stderr,
-                 "pk trace (us): total %.1f  P0 %.1f  XF %.1f  Y %.1f  Z %.1f  YI %.1f  XI %.1f  last+sum %.1f "
-                 "(grid %d)\n",
-                 (ts[5 * k + 3] - ts[0]) * 1e-3, ph[0] * 1e-3, ph[1] * 1e-3, ph[2] * 1e-3, ph[3] * 1e-3,
-                 ph[4] * 1e-3, ph[5] * 1e-3, ph[6] * 1e-3, c->pk_grid);
+      for (int p = 0; p < P; ++p) ph[1 + p] += (double)(ts[2 + P * j + p] - ts[1 + P * j + p]);
+    ph[6] = (double)(ts[P * k + 3] - ts[P * k + 1]);
+    std::fprintf(stderr, "pk trace (us): total %.1f  P0 %.1f ", (ts[P * k + 3] - ts[0]) * 1e-3, ph[0] * 1e-3);
+    for (int p = 0; p < P; ++p) std::fprintf(stderr, " %s %.1f", names[p], ph[1 + p] * 1e-3);
+    std::fprintf(stderr, "  last+sum %.1f (grid %d)\n", ph[6] * 1e-3, c->pk_grid);
     if (trace_ctas) {
       // per phase type: CTA work time (arrival - own previous release),
       // median and max over CTAs and steps; arrival spread (last - first
@@ -1332,12 +1335,11 @@ bool coarse_pk_run(rism3d_ctx *c, int k) {
       const int G = c->pk_grid;
       std::vector<unsigned long long> tc((size_t)nbar * 2 * G);
       CK(cudaMemcpy(tc.data(), c->pk_trace_cta, sizeof(unsigned long long) * tc.size(), cudaMemcpyDeviceToHost));
-      const char *names[5] = {"XF", "Y", "Z", "YI", "XI"};
-      for (int p = 0; p < 5; ++p) {
+      for (int p = 0; p < P; ++p) {
         std::vector<double> work;
         double spread = 0, lag = 0, lagmax = 0;
         for (int j = 0; j < k; ++j) {
-          const int b = 1 + 5 * j + p;  // barrier index (0-based) closing this phase
+          const int b = 1 + P * j + p;  // barrier index (0-based) closing this phase
           unsigned long long amin = ~0ull, amax = 0, rmax = 0;
           for (int q = 0; q < G; ++q) {
             const unsigned long long arr = tc[(size_t)b * 2 * G + q], prev = tc[(size_t)(b - 1) * 2 * G + G + q];
@@ -1359,7 +1361,7 @@ bool coarse_pk_run(rism3d_ctx *c, int k) {
     if (trace_steps) {
       for (int j = 0; j < k; ++j) {
         std::fprintf(stderr, "  step %2d:", j);
-        for (int p = 0; p < 5; ++p) std::fprintf(stderr, " %6.2f", (ts[2 + 5 * j + p] - ts[1 + 5 * j + p]) * 1e-3);
+        for (int p = 0; p < P; ++p) std::fprintf(stderr, " %6.2f", (ts[2 + P * j + p] - ts[1 + P * j + p]) * 1e-3);
         std::fprintf(stderr, "\n");
       }
     }
