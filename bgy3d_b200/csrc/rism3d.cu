@@ -890,9 +890,38 @@ template <typename TS> __global__ void k_slope_any(long long n, const TS *__rest
   if (d64) d64[p] = d;
 }
 
+// The FP32 Jacobian's slope from an FP32 state: FP32 arithmetic on the
+// FP32 potential (the one the FP32 residual passes use), four elements per
+// thread; the FP64 potential and FP64 exponentials were most of
+// k_slope_any's time and are lost in the FP32 result anyway.
+__global__ void k_slope_f32(long long n, const float *__restrict__ t, const float *__restrict__ v, float beta,
+                            int closure, float *__restrict__ d) {
+  const long long n4 = n / 4;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += (long long)gridDim.x * blockDim.x) {
+    const float4 tv = reinterpret_cast<const float4 *>(t)[q], vv = reinterpret_cast<const float4 *>(v)[q];
+    float4 o;
+    o.x = closure_d<float>(closure, beta * vv.x, tv.x);
+    o.y = closure_d<float>(closure, beta * vv.y, tv.y);
+    o.z = closure_d<float>(closure, beta * vv.z, tv.z);
+    o.w = closure_d<float>(closure, beta * vv.w, tv.w);
+    reinterpret_cast<float4 *>(d)[q] = o;
+  }
+  if (blockIdx.x == 0 && threadIdx.x < (unsigned)(n - 4 * n4)) {
+    const long long p = 4 * n4 + threadIdx.x;
+    d[p] = closure_d<float>(closure, beta * v[p], t[p]);
+  }
+}
+
 template <typename TS, typename TJ> void closure_slope(rism3d_ctx *c, const TS *x, TJ *d) {
   TimeScope ts(c, TK_VEC, sizeof(TJ) == 8 ? 0 : 1);
   const long long n = c->nvec;
+  if constexpr (sizeof(TS) == 4 && sizeof(TJ) == 4) {
+    if (c->v32 && (reinterpret_cast<uintptr_t>(x) & 15) == 0 && (reinterpret_cast<uintptr_t>(d) & 15) == 0) {
+      k_slope_f32<<<vec_grid(n / 4 + 1), 256, 0, c->stream>>>(n, x, c->v32, (float)c->pd.beta, c->pd.closure, d);
+      CKL();
+      return;
+    }
+  }
   float *d32 = sizeof(TJ) == 4 ? reinterpret_cast<float *>(d) : nullptr;
   double *d64 = sizeof(TJ) == 8 ? reinterpret_cast<double *>(d) : nullptr;
   k_slope_any<TS><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, x, c->v64, c->pd.beta, c->pd.closure,
