@@ -168,25 +168,31 @@ __global__ void __launch_bounds__(256) k_maxpyv(long long nw, T *__restrict__ w,
   }
 }
 
-// out[v] = sum_b part[b * stride + v] for v < nv: one block of kVecMax x 8
-// threads, each summing every 8th partial, then a fixed-order combine.
-__global__ static void __launch_bounds__(kVecMax * 8) k_colsum(int nblk, int stride, int nv,
-                                                              const double *__restrict__ part,
-                                                              double *__restrict__ out) {
-  const int v = threadIdx.x % kVecMax, j = threadIdx.x / kVecMax;
-  __shared__ double sm[8][kVecMax];
+// out[v] = sum_b part[b * stride + v] for v < nv (<= kVecMax): one block of
+// kColsumThreads as (v, group) lanes, lanes = the power of two >= nv; group
+// q sums every groups-th partial, then a pairwise tree over the groups (a
+// fixed order).  With few vectors most of the block's threads take part
+// instead of eight per vector.
+constexpr int kColsumThreads = 1024;
+__global__ static void __launch_bounds__(kColsumThreads) k_colsum(int nblk, int stride, int nv,
+                                                                 const double *__restrict__ part,
+                                                                 double *__restrict__ out) {
+  __shared__ double red[kColsumThreads];
+  int lanes = 1;
+  while (lanes < nv) lanes <<= 1;
+  const int groups = kColsumThreads / lanes;
+  const int t = threadIdx.x, v = t % lanes, q = t / lanes;
   double a = 0.0;
   if (v < nv)
 #pragma unroll 4
-    for (int b = j; b < nblk; b += 8) a += part[(long long)b * stride + v];
-  sm[j][v] = a;
+    for (int b = q; b < nblk; b += groups) a += part[(long long)b * stride + v];
+  red[t] = a;
   __syncthreads();
-  if (j == 0 && v < nv) {
-    double s = 0.0;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) s += sm[q][v];
-    out[v] = s;
+  for (int st = kColsumThreads / 2; st >= lanes; st >>= 1) {
+    if (t < st) red[t] += red[t + st];
+    __syncthreads();
   }
+  if (t < nv) out[t] = red[t];
 }
 
 // w /= sqrt(*nrm2) (w = 0 when the norm is 0); the norm goes to *hout.

@@ -686,7 +686,7 @@ void mdot(rism3d_ctx *c, const T *w, double ws, const std::vector<VecRef<T>> &V,
     for (int i = 0; i < kVecMax; ++i) vs.p[i] = V[base + (i < k ? i : 0)].p;
     launch_mdotv<T>(G, c->stream, nw, w, k, vs, c->dpart);
     CKL();
-    k_colsum<<<1, kVecMax * 8, 0, c->stream>>>(G, kVecMax, k, c->dpart, c->dres + base);
+    k_colsum<<<1, kColsumThreads, 0, c->stream>>>(G, kVecMax, k, c->dpart, c->dres + base);
     CKL();
   }
   double *hres = pinned_scratch();
@@ -718,7 +718,7 @@ double maxpy(rism3d_ctx *c, T *w, double ws, const std::vector<VecRef<T>> &V, co
     CKL();
   }
   if (!want_norm) return 0.0;
-  k_colsum<<<1, kVecMax * 8, 0, c->stream>>>(G, 1, 1, c->dpart, c->dres);
+  k_colsum<<<1, kColsumThreads, 0, c->stream>>>(G, 1, 1, c->dpart, c->dres);
   CKL();
   double *hres = pinned_scratch();
   CK(cudaMemcpyAsync(hres, c->dres, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -745,11 +745,11 @@ double gs_step(rism3d_ctx *c, T *w, const std::vector<VecRef<T>> &V, std::vector
   }
   launch_mdotv<T>(G, c->stream, nw, w, nv, vs, c->dpart);
   CKL();
-  k_colsum<<<1, kVecMax * 8, 0, c->stream>>>(G, kVecMax, nv, c->dpart, c->dres);
+  k_colsum<<<1, kColsumThreads, 0, c->stream>>>(G, kVecMax, nv, c->dpart, c->dres);
   CKL();
   launch_maxpyv<T>(G, c->stream, nw, w, 1.0, nv, vs, cf, c->dres, c->dpart);
   CKL();
-  k_colsum<<<1, kVecMax * 8, 0, c->stream>>>(G, 1, 1, c->dpart, c->dres + kVecMax);
+  k_colsum<<<1, kColsumThreads, 0, c->stream>>>(G, 1, 1, c->dpart, c->dres + kVecMax);
   CKL();
   double *hres = pinned_scratch();
   CK(cudaMemcpyAsync(hres, c->dres, sizeof(double) * (kVecMax + 1), cudaMemcpyDeviceToHost, c->stream));
@@ -782,9 +782,10 @@ template <typename T> void ensure_basis(rism3d_ctx *c, int count) {
 
 // GMRES(restart) without preconditioner for J x = b, x0 = 0 (KSPGMRES with
 // classical Gram-Schmidt, PCNONE; bgy3d-snes.c:262-306).  Returns the
-// number of J.v products.  b is overwritten.
+// number of J.v products.  b is only read: the first cycle's basis starts
+// from b in place.
 template <typename T>
-int gmres(rism3d_ctx *c, const T *d, T *b, T *x, double rtol, int maxit, int restart) {
+int gmres(rism3d_ctx *c, const T *d, const T *b, T *x, double rtol, int maxit, int restart) {
   ensure_basis<T>(c, restart + 1);
   auto &B = basis<T>(c);
   std::vector<double> H((size_t)(restart + 1) * restart), cs(restart), sn(restart), gv(restart + 1);
@@ -795,22 +796,19 @@ int gmres(rism3d_ctx *c, const T *d, T *b, T *x, double rtol, int maxit, int res
   double beta0 = -1.0;
   while (its < maxit) {
     // r = b - J x (first cycle: r = b)
-    double resid[2];
-    if (!have_x) {
-      axpby<T, T>(c, 1.0, b, 0.0, B[0]);
-      V.assign(1, vref<T>(B[0], 1.0));
-      const double nb = maxpy<T>(c, B[0], 1.0, {}, {}, true);
-      resid[1] = nb;
-    } else {
+    // r0 = b in the first cycle (read in place: the norm-only sweep writes
+    // nothing), else B0 = b - J x
+    T *r0 = const_cast<T *>(b);
+    if (have_x) {
       eval_J<T>(c, d, x, 1.0, B[0], nullptr);  // B0 = J x
       xpay<T, T, T>(c, b, -1.0, B[0], B[0]);   // B0 = b - J x
-      resid[1] = maxpy<T>(c, B[0], 1.0, {}, {}, true);
+      r0 = B[0];
       its++;
     }
-    const double beta = resid[1];
+    const double beta = maxpy<T>(c, r0, 1.0, {}, {}, true);
     if (beta0 < 0) beta0 = beta;
     if (beta == 0.0 || beta <= rtol * beta0) break;
-    V.assign(1, vref<T>(B[0], 1.0 / beta));
+    V.assign(1, vref<T>(r0, 1.0 / beta));
     std::fill(gv.begin(), gv.end(), 0.0);
     gv[0] = beta;
     int j = 0;
@@ -1146,7 +1144,7 @@ void coarse_solve_dev(rism3d_ctx *c, int k) {
   Coefs one{}, mone{};
   for (int i = 0; i < kVecMax; ++i) one.c[i] = 1.0, mone.c[i] = -1.0;
   launch_maxpyv<float>(G, st, nw, B[0], 1.0, 0, VecSet<float>{}, one, nullptr, cc->dpart);
-  k_colsum<<<1, kVecMax * 8, 0, st>>>(G, 1, 1, cc->dpart, nrm);  // |r|^2
+  k_colsum<<<1, kColsumThreads, 0, st>>>(G, 1, 1, cc->dpart, nrm);  // |r|^2
   k_scale_norm<float><<<gv, 256, 0, st>>>(cc->nvec, B[0], nrm, beta);
   CKL();
   for (int j = 0; j < k; ++j) {
@@ -1444,7 +1442,7 @@ template <> std::vector<float *> &zbasis<float>(rism3d_ctx *c) { return c->zbasi
 // Comput. 14 (1993) 461).  Classical Gram-Schmidt as in gmres(); returns
 // the number of fine J.v products.
 template <typename T>
-int fgmres(rism3d_ctx *c, const T *d, T *b, T *x, double rtol, int maxit, int restart) {
+int fgmres(rism3d_ctx *c, const T *d, const T *b, T *x, double rtol, int maxit, int restart) {
   auto &B = basis<T>(c);
   auto &Z = zbasis<T>(c);
   ensure_basis<T>(c, 1);
@@ -1455,17 +1453,19 @@ int fgmres(rism3d_ctx *c, const T *d, T *b, T *x, double rtol, int maxit, int re
   double beta0 = -1.0;
   int its = 0;
   while (its < maxit) {
-    if (!have_x) {
-      axpby<T, T>(c, 1.0, b, 0.0, B[0]);
-    } else {
+    // r0 = b in the first cycle (read in place: the norm-only sweep writes
+    // nothing), else B0 = b - J x
+    T *r0 = const_cast<T *>(b);
+    if (have_x) {
       eval_J<T>(c, d, x, 1.0, B[0], nullptr);  // B0 = J x
       its++;
       xpay<T, T, T>(c, b, -1.0, B[0], B[0]);   // B0 = b - J x
+      r0 = B[0];
     }
-    const double beta = maxpy<T>(c, B[0], 1.0, {}, {}, true);
+    const double beta = maxpy<T>(c, r0, 1.0, {}, {}, true);
     if (beta0 < 0) beta0 = beta;
     if (beta == 0.0 || beta <= rtol * beta0) break;
-    V.assign(1, vref<T>(B[0], 1.0 / beta));
+    V.assign(1, vref<T>(r0, 1.0 / beta));
     std::fill(gv.begin(), gv.end(), 0.0);
     gv[0] = beta;
     int j = 0;
@@ -1537,16 +1537,24 @@ template <typename TS, typename TJ>
 NewtonOut newton(rism3d_ctx *c, TS *x, double tol, int max_iter, double krylov_rtol, int restart,
                  double eta0 = 0.5) {
   NewtonOut o;
+  // An accepted step swaps the state with the trial and the residual with
+  // the trial residual (pointers, not copies); the state ends in x.
+  TS *xc = x;
   TS *F = xbuf<TS>(c, 0);
   TS *xt = xbuf<TS>(c, 1);
   TS *Ft = xbuf<TS>(c, 2);
   TJ *d = slopebuf<TJ>(c);
   TJ *dx = dxbuf<TJ>(c);
-  // -F in the Jacobian precision: Ft doubles as scratch when TS == TJ,
-  // otherwise the (idle) FP32 trial buffer
-  TJ *rhs = xbuf<TJ>(c, sizeof(TJ) == sizeof(TS) ? 2 : 1);
+  // -F in the Jacobian precision where that differs from the state's (the
+  // idle FP32 trial buffer); otherwise the Krylov solve reads F itself and
+  // the step is taken with the opposite sign: a solve from zero is odd in
+  // its right-hand side, bitwise (negation is exact, every operation
+  // sign-symmetric), so dx(F) = -dx(-F)
+  constexpr bool same = sizeof(TJ) == sizeof(TS);
+  TJ *rhs = same ? nullptr : xbuf<TJ>(c, 1);
+  const double sg = same ? -1.0 : 1.0;
   double r[2];
-  eval_F<TS>(c, x, F, r);
+  eval_F<TS>(c, xc, F, r);
   // Eisenstat-Walker forcing (PETSc's version 2: gamma 0.9, alpha 2,
   // safeguard above 0.1), floored at the reference's fixed KSP rtol and
   // never below what the last step needs to reach tol.
@@ -1577,21 +1585,27 @@ NewtonOut newton(rism3d_ctx *c, TS *x, double tol, int max_iter, double krylov_r
     // iterations are cheap, so those solves are held to 0.1.
     if (c->coarse) eta_use = std::min(eta_use, 0.1);
     r2_prev = r[1];
-    closure_slope<TS, TJ>(c, x, d);
-    axpby<TS, TJ>(c, -1.0, F, 0.0, rhs);
+    closure_slope<TS, TJ>(c, xc, d);
+    const TJ *b;
+    if constexpr (same) {
+      b = F;
+    } else {
+      axpby<TS, TJ>(c, -1.0, F, 0.0, rhs);
+      b = rhs;
+    }
     int kits;
     if (c->coarse) {
       tg_prepare<TJ>(c, d);
-      kits = fgmres<TJ>(c, d, rhs, dx, eta_use, 1000, restart);
+      kits = fgmres<TJ>(c, d, b, dx, eta_use, 1000, restart);
     } else {
-      kits = gmres<TJ>(c, d, rhs, dx, eta_use, 1000, restart);
+      kits = gmres<TJ>(c, d, b, dx, eta_use, 1000, restart);
     }
     if (c->pd.verbosity > 0) std::fprintf(stderr, "   gmres: %d J.v (rtol %.2e)\n", kits, eta_use);
     const double f0 = r[1] * r[1];
     double lam = 1.0, f1 = 0.0, rt[2] = {0, 0};
     bool decreased = false;
     for (int ls = 0; ls < 20; ++ls) {
-      xpay<TS, TJ, TS>(c, x, lam, dx, xt);
+      xpay<TS, TJ, TS>(c, xc, sg * lam, dx, xt);
       eval_F<TS>(c, xt, Ft, rt);
       f1 = rt[1] * rt[1];
       if (f1 <= (1.0 - 2e-4 * lam) * f0) { decreased = true; break; }
@@ -1604,12 +1618,13 @@ NewtonOut newton(rism3d_ctx *c, TS *x, double tol, int max_iter, double krylov_r
       o.stalled = true;
       break;
     }
-    // accept: x <- xt, F <- Ft
-    axpby<TS, TS>(c, 1.0, xt, 0.0, x);
-    axpby<TS, TS>(c, 1.0, Ft, 0.0, F);
+    // accept: the trial becomes the state, its residual the residual
+    std::swap(xc, xt);
+    std::swap(F, Ft);
     r[0] = rt[0];
     r[1] = rt[1];
   }
+  if (xc != x) axpby<TS, TS>(c, 1.0, xc, 0.0, x);
   return o;
 }
 
