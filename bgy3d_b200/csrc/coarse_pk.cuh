@@ -151,7 +151,8 @@ __device__ __forceinline__ void pk_block_sum(double s, double *part) {
 }
 
 // The split of the x-phase transforms (measured: the larger first radix of
-// Split beats SplitRow at 48-row items of 32-point rows).
+// Split beats SplitRow at 48-row items of 32-point rows, and ties with it at
+// the plane form's 64-row items).
 template <int M> using PkSplit = Split<M>;
 
 // Rows of the x phases per work item: about one item per CTA of a 2 x 148
@@ -426,12 +427,19 @@ __device__ __forceinline__ void pk_y(const PkArgs &a, float2 *smem, const float2
 }
 
 // Z: the three site tiles [N][4] of one (kx block, ky) transformed as one
-// 12-column tile, the OZ contraction, the inverse.
+// 12-column tile, the OZ contraction, the inverse.  The z transforms split
+// N = R1 R2 with R1 about sqrt(N) (64 = 8 x 8): every thread of a group has
+// one DFT of each step, and a thread holds half the values of the 16 x 4
+// split.
 constexpr int kPkBz = 4;
+template <int N> struct PkZSplit {
+  static constexpr int R1 = N == 48 ? 8 : N == 64 ? 8 : N == 72 ? 8 : N == 96 ? 12 : N == 128 ? 16 : Split<N>::R1;
+  static constexpr int R2 = N / R1;
+};
 template <int N>
 __device__ __forceinline__ void pk_z(const PkArgs &a, float2 *smem, const float2 *tw) {
   constexpr int B = kPkBz, MS = 3;
-  constexpr int NG = Split<N>::R1 * B * MS;
+  constexpr int NG = PkZSplit<N>::R1 * B * MS;
   constexpr int GPC = kPkThreads / NG;
   static_assert(GPC >= 1, "a z tile needs at most one CTA of threads");
   const Geo &g = a.g;
@@ -456,7 +464,7 @@ __device__ __forceinline__ void pk_z(const PkArgs &a, float2 *smem, const float2
       }
     }
     __syncthreads();
-    z_tile_g<float, MODE_J, N, B, MS, true, 1>(g, buf, tw, a.zp, kx0, y, tid, act);
+    z_tile_g<float, MODE_J, N, B, MS, true, 1, PkZSplit<N>>(g, buf, tw, a.zp, kx0, y, tid, act);
     if (act) {
       for (int e = tid; e < g.m * N * (B / 2); e += NG) {
         const int s = e / (N * (B / 2)), r = e % (N * (B / 2));
@@ -508,7 +516,7 @@ template <int M, int N, bool PLANE = false> __host__ __device__ constexpr size_t
   constexpr size_t xs = PLANE ? (size_t)N * (LayRow<M, PkSplit<M>::R2>::RS + pk_ncp<M>())
                               : (size_t)pk_rx<M>() * LayRow<M, PkSplit<M>::R2>::RS;
   constexpr size_t ys = PLANE ? 0 : (size_t)(kPkThreads / (Split<N>::R1 * 16)) * N * 16;
-  constexpr size_t zs = (size_t)(kPkThreads / (Split<N>::R1 * kPkBz * 3)) * 3 * N * kPkBz;
+  constexpr size_t zs = (size_t)(kPkThreads / (PkZSplit<N>::R1 * kPkBz * 3)) * 3 * N * kPkBz;
   constexpr size_t tile = xs > ys ? (xs > zs ? xs : zs) : (ys > zs ? ys : zs);
   return sizeof(float2) * (M + 2 * N + tile);
 }

@@ -293,12 +293,13 @@ template <typename T, int MODE> __host__ __device__ constexpr int zpf_default() 
 // while it contracts the current one, and issues the first ZPF before the
 // forward transforms, under whose latency they arrive.  Same arithmetic in
 // the same order as contracting element by element.
-template <typename T, int MODE, int N, int B, int MS, bool JOINT = false, int ZPF = zpf_default<T, MODE>()>
+template <typename T, int MODE, int N, int B, int MS, bool JOINT = false, int ZPF = zpf_default<T, MODE>(),
+          class S = Split<N>>
 __device__ __forceinline__ void z_tile_g(const Geo &g, typename Cx<T>::type *buf, const typename Cx<T>::type *tw,
                                          const ZParams<T> &zp, int kx0, int y, int tid, bool act) {
   using V = typename Cx<T>::type;
   using P2 = typename Vec2<T>::type;
-  constexpr int NTHR = Split<N>::R1 * B * (JOINT ? MS : 1);
+  constexpr int NTHR = S::R1 * B * (JOINT ? MS : 1);
   constexpr int NP = MS * (MS + 1) / 2;
   constexpr int NIT = (N * B + NTHR - 1) / NTHR;
   constexpr int D = NIT < ZPF ? NIT : ZPF;
@@ -341,9 +342,9 @@ __device__ __forceinline__ void z_tile_g(const Geo &g, typename Cx<T>::type *buf
   };
 #pragma unroll
   for (int s = 0; s < D; ++s) fetch(s, s);
-  if (JOINT) fft2g<N, MS * B, NTHR, false, true, LayCol<N, B>>(buf, tw, tid, act);
+  if (JOINT) fft2g<N, MS * B, NTHR, false, true, LayCol<N, B>, S>(buf, tw, tid, act);
   else
-    for (int s = 0; s < m; ++s) fft2g<N, B, NTHR, false, true, LayCol<N, B>>(buf + s * N * B, tw, tid, act);
+    for (int s = 0; s < m; ++s) fft2g<N, B, NTHR, false, true, LayCol<N, B>, S>(buf + s * N * B, tw, tid, act);
 #pragma unroll
   for (int it = 0; it < NIT; ++it) {
     const int slot = it % D;
@@ -392,9 +393,9 @@ __device__ __forceinline__ void z_tile_g(const Geo &g, typename Cx<T>::type *buf
     if (it + D < NIT) fetch(it + D, slot);
   }
   __syncthreads();
-  if (JOINT) fft2g<N, MS * B, NTHR, true, true, LayCol<N, B>>(buf, tw, tid, act);
+  if (JOINT) fft2g<N, MS * B, NTHR, true, true, LayCol<N, B>, S>(buf, tw, tid, act);
   else
-    for (int s = 0; s < m; ++s) fft2g<N, B, NTHR, true, true, LayCol<N, B>>(buf + s * N * B, tw, tid, act);
+    for (int s = 0; s < m; ++s) fft2g<N, B, NTHR, true, true, LayCol<N, B>, S>(buf + s * N * B, tw, tid, act);
 }
 template <typename T, int MODE, int N, int B, int MS>
 __device__ __forceinline__ void z_tile(const Geo &g, typename Cx<T>::type *buf, const typename Cx<T>::type *tw,
