@@ -273,7 +273,7 @@ __device__ __forceinline__ void pk_xf(const PkArgs &a, float *const *V, int j, i
     }
     __syncthreads();  // buf is refilled by the next item
     if constexpr (PLANE) {
-      fft2g<N, M + 1, kPkThreads, false, true, LayCol<N, NCP>>(T, twy, tid, true);
+      fft2g<N, M + 1, kPkThreads, false, true, LayCol<N, NCP>, SplitSq<N>>(T, twy, tid, true);
       float4 *dst = reinterpret_cast<float4 *>(a.W + (long long)item * N * NCP);
       const float4 *src = reinterpret_cast<const float4 *>(T);
       for (int e = tid; e < N * NCP / 2; e += kPkThreads) dst[e] = src[e];
@@ -319,7 +319,7 @@ __device__ __forceinline__ void pk_xi(const PkArgs &a, float *const *V, int j, f
       float4 *dst = reinterpret_cast<float4 *>(T);
       for (int e = tid; e < N * NCP / 2; e += kPkThreads) dst[e] = src[e];
       __syncthreads();
-      fft2g<N, M + 1, kPkThreads, true, true, LayCol<N, NCP>>(T, twy, tid, true);
+      fft2g<N, M + 1, kPkThreads, true, true, LayCol<N, NCP>, SplitSq<N>>(T, twy, tid, true);
     }
     for (int e = tid; e < RX * H; e += kPkThreads) {
       const int row = e / H, kk = e % H;
@@ -432,10 +432,7 @@ __device__ __forceinline__ void pk_y(const PkArgs &a, float2 *smem, const float2
 // one DFT of each step, and a thread holds half the values of the 16 x 4
 // split.
 constexpr int kPkBz = 4;
-template <int N> struct PkZSplit {
-  static constexpr int R1 = N == 48 ? 8 : N == 64 ? 8 : N == 72 ? 8 : N == 96 ? 12 : N == 128 ? 16 : Split<N>::R1;
-  static constexpr int R2 = N / R1;
-};
+template <int N> using PkZSplit = SplitSq<N>;
 template <int N>
 __device__ __forceinline__ void pk_z(const PkArgs &a, float2 *smem, const float2 *tw) {
   constexpr int B = kPkBz, MS = 3;

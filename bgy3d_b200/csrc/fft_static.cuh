@@ -82,6 +82,15 @@ template <int N> struct Split {
   static constexpr int R2 = N / R1;
 };
 
+// A split with R1 near sqrt(N) (64 = 8 x 8, 96 = 12 x 8): where a tile has
+// few columns, Split's larger first radix leaves most threads of a step idle
+// (16 x 4 over 16 columns: 64 DFTs for 256 threads) and holds twice the
+// values per thread.
+template <int N> struct SplitSq {
+  static constexpr int R1 = N == 48 ? 8 : N == 64 ? 8 : N == 72 ? 8 : N == 96 ? 12 : N == 128 ? 16 : Split<N>::R1;
+  static constexpr int R2 = N / R1;
+};
+
 // The split of the row-batched transforms (x passes and x transfers: one
 // work item per row and index, COLFAST false), where Split's larger first
 // radix would leave most of the CTA idle in one step (32 = 16 x 2 gives R2 x

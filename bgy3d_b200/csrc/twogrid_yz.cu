@@ -59,7 +59,9 @@ __global__ void __launch_bounds__(256) k_transfer_fft(int outer, int inner, cons
                               : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  fft2<NI, B, 256, false, true, LayCol<NI, B>>(X, ti);
+  // square splits: over 16 columns the 16 x 4 split of 64 points leaves
+  // three quarters of the threads idle in its first step
+  fft2<NI, B, 256, false, true, LayCol<NI, B>, SplitSq<NI>>(X, ti);
   const float scale = 1.0f / (float)NI;
   for (int e = tid; e < NO * B; e += 256) {
     const int k = e / B, c = e - k * B;
@@ -86,7 +88,7 @@ __global__ void __launch_bounds__(256) k_transfer_fft(int outer, int inner, cons
     Y[e] = make_float2(v.x * scale, v.y * scale);
   }
   __syncthreads();
-  fft2<NO, B, 256, true, true, LayCol<NO, B>>(Y, to);
+  fft2<NO, B, 256, true, true, LayCol<NO, B>, SplitSq<NO>>(Y, to);
   float *dst = out + (long long)o * NO * inner + i0;
   for (int e = tid; e < NO * B; e += 256) {
     const int k = e / B, c = e - k * B;
