@@ -659,6 +659,30 @@ __global__ void k_closure_slope(long long n, long long Nr, const double *__restr
 // densities by the native, HNC, KH and GF functionals and of c; g = h + 1.
 struct ObsPartial { double mu, hnc, kh, gf, csum; };
 
+// out[0..4] = the sums of the five fields of part[0..nblk): one block of
+// 1024 threads, strided per thread, then a pairwise tree (a fixed order).
+__global__ static void __launch_bounds__(1024) k_obs_final(int nblk, const ObsPartial *__restrict__ part,
+                                                           double *__restrict__ out) {
+  __shared__ double red[5][1024];
+  const int t = threadIdx.x;
+  double a[5] = {0, 0, 0, 0, 0};
+  for (int b = t; b < nblk; b += 1024) {
+    const ObsPartial p = part[b];
+    a[0] += p.mu; a[1] += p.hnc; a[2] += p.kh; a[3] += p.gf; a[4] += p.csum;
+  }
+#pragma unroll
+  for (int q = 0; q < 5; ++q) red[q][t] = a[q];
+  __syncthreads();
+  for (int st = 512; st > 0; st >>= 1) {
+    if (t < st) {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) red[q][t] += red[q][t + st];
+    }
+    __syncthreads();
+  }
+  if (t < 5) out[t] = red[t][0];
+}
+
 static __global__ void k_observables(Geo g, const double *__restrict__ t, const double *__restrict__ v,
                               const double *__restrict__ uc, double beta, int closure,
                               const double *__restrict__ charge, double *__restrict__ gout,
